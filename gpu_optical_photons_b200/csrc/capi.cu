@@ -1,0 +1,906 @@
+// capi.cu - the extern "C" boundary of liboptx.so (declared in include/optx.h).
+//
+// Host side of the engine: argument checks with the reference's error
+// behaviour (invalid_argument -> OPTX_ERR_INVALID_ARGUMENT, runtime_error ->
+// OPTX_ERR_RUNTIME, CUDA_CHECK -> OPTX_ERR_CUDA; src/gpu/gpu_event.cu:177-182,
+// src/gpu/gpu_backend.cu:171-185, src/gpu/cuda_util.cuh:17-24 of the reference),
+// conversion of SimParams into the kernels' DevParams, cached device buffers,
+// timing with CUDA events, and the wavefront engine object (state queues,
+// control block, CUDA-graph while loop).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/optx.h"
+#include "optx_device.cuh"
+#include "optx_engine.hpp"
+
+using namespace optx;
+
+namespace {
+
+thread_local std::string g_err;
+std::mutex g_mu;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define OPTX_CUDA(call)                                                                   \
+  do {                                                                                    \
+    const cudaError_t err_ = (call);                                                      \
+    if (err_ != cudaSuccess) {                                                            \
+      return fail(OPTX_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(err_) + \
+                                     " at " __FILE__ ":" + std::to_string(__LINE__) +     \
+                                     " (" #call ")");                                     \
+    }                                                                                     \
+  } while (0)
+
+#define OPTX_TRY(call)            \
+  do {                            \
+    const int rc_ = (call);       \
+    if (rc_ != OPTX_OK) return rc_; \
+  } while (0)
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+constexpr float kSpeedOfLight = 299.792458f;  // mm/ns (hd.hpp:37 of the reference)
+
+int check_params(const optx_params* p, const optx_faces* f) {
+  if (p == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "params must not be NULL");
+  if (!(p->hx > 0.0f && p->hy > 0.0f && p->hz > 0.0f) || !std::isfinite(p->hx) ||
+      !std::isfinite(p->hy) || !std::isfinite(p->hz))
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "box half-sizes must be positive and finite");
+  if (!(p->n_scint > 0.0f && p->n_det > 0.0f && p->n_out > 0.0f))
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "refractive indices must be positive");
+  if (!(p->abs_length > 0.0f) || !(p->scat_length > 0.0f))
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "abs_length and scat_length must be > 0 (inf disables)");
+  if (p->surface > 3u) return fail(OPTX_ERR_INVALID_ARGUMENT, "surface must be 0..3");
+  if (p->source > 1u) return fail(OPTX_ERR_INVALID_ARGUMENT, "source must be 0 (point) or 1 (volume)");
+  if (!(p->tau >= 0.0f) || !std::isfinite(p->tau))
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "tau must be finite and >= 0");
+  if (f != nullptr) {
+    for (int i = 0; i < 5; ++i)
+      if (f->surface[i] > 3u) return fail(OPTX_ERR_INVALID_ARGUMENT, "face surface must be 0..3");
+  }
+  return OPTX_OK;
+}
+
+// SimParams (+ optional per-face surfaces) -> the kernels' 112-byte record. The
+// derived quantities use the reference's float expressions: inv_speed =
+// n_scint / c (transport.hpp:74), eta = n1 / n2 and eta * eta (fresnel.hpp:32-33).
+DevParams make_dev_params(const optx_params& p, const optx_faces* f) {
+  DevParams d;
+  std::memset(&d, 0, sizeof(d));
+  d.hx = p.hx;
+  d.hy = p.hy;
+  d.hz = p.hz;
+  volatile float ns = p.n_scint;  // keep the host division in float
+  d.inv_speed = ns / kSpeedOfLight;
+  d.n_scint = p.n_scint;
+  d.n_det = p.n_det;
+  d.n_out = p.n_out;
+  d.abs_length = p.abs_length;
+  d.scat_length = p.scat_length;
+  d.tau = p.tau;
+  d.src_x = p.src_x;
+  d.src_y = p.src_y;
+  d.src_z = p.src_z;
+  uint32_t bits = 0;
+  float refl[5];
+  for (int i = 0; i < 5; ++i) {
+    const uint32_t m = f ? f->surface[i] : p.surface;
+    bits |= (m & 3u) << (2 * i);
+    refl[i] = f ? f->reflectivity[i] : p.reflectivity;
+  }
+  d.surf_bits = bits;
+  d.refl0 = refl[0];
+  d.refl1 = refl[1];
+  d.refl2 = refl[2];
+  d.refl3 = refl[3];
+  d.refl4 = refl[4];
+  d.max_steps = p.max_steps;
+  d.source = p.source;
+  volatile float e1 = p.n_scint / p.n_det;
+  volatile float e2 = p.n_scint / p.n_out;
+  d.eta2_det = e1 * e1;
+  d.eta2_out = e2 * e2;
+  d.key_lo = static_cast<uint32_t>(p.seed);
+  d.key_hi = static_cast<uint32_t>(p.seed >> 32);
+  return d;
+}
+
+int make_tally_dev(const optx_tally_config* c, TallyDev& t) {
+  if (c == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "tally config must not be NULL");
+  if (c->time_bins == 0u || c->xy_bins == 0u || !(c->time_max > 0.0f))
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "tally config needs time_bins, xy_bins >= 1, time_max > 0");
+  const uint64_t len = 5ull + c->time_bins + 1ull + static_cast<uint64_t>(c->xy_bins) * c->xy_bins + 2ull;
+  if (len > (1ull << 30)) return fail(OPTX_ERR_INVALID_ARGUMENT, "tally too large");
+  t.time_bins = c->time_bins;
+  volatile float tb = static_cast<float>(c->time_bins);
+  t.tscale = tb / c->time_max;  // transport.hpp:171
+  t.xy_bins = c->xy_bins;
+  t.len = static_cast<uint32_t>(len);
+  return OPTX_OK;
+}
+
+int check_block(int block) {
+  if (block <= 0 || block % 32 != 0 || block > 1024)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 <= 1024");
+  return OPTX_OK;
+}
+
+int check_math(int math) {
+  if (math != OPTX_MATH_FAST && math != OPTX_MATH_EXACT)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "math must be OPTX_MATH_FAST or OPTX_MATH_EXACT");
+  return OPTX_OK;
+}
+
+int ensure_device() {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(OPTX_ERR_NO_DEVICE, "no CUDA device available");
+  }
+  OPTX_CUDA(cudaFree(nullptr));  // context creation outside the timed region (cuda_util.cuh:63-65)
+  return OPTX_OK;
+}
+
+int num_sms() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n > 0 ? n : 1;
+}
+
+// ---- math-mode dispatch -------------------------------------------------------
+#define DISPATCH(math, fn, ...) ((math) == OPTX_MATH_EXACT ? exact::fn(__VA_ARGS__) : fast::fn(__VA_ARGS__))
+
+// ---- cached device buffers (per process; the library serialises calls) ---------
+struct Cache {
+  void* rec = nullptr;
+  size_t rec_bytes = 0;
+  unsigned long long* tally = nullptr;
+  size_t tally_bytes = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+Cache g_cache;
+
+int cache_events() {
+  if (g_cache.e0 == nullptr) {
+    OPTX_CUDA(cudaEventCreate(&g_cache.e0));
+    OPTX_CUDA(cudaEventCreate(&g_cache.e1));
+  }
+  return OPTX_OK;
+}
+
+int cache_records(size_t cap, DevRecords& d) {
+  const size_t bytes = cap * (1 + 4 + 4 + 5 * 4) + 8 * 256;
+  if (g_cache.rec_bytes < bytes) {
+    if (g_cache.rec) cudaFree(g_cache.rec);
+    g_cache.rec = nullptr;
+    g_cache.rec_bytes = 0;
+    OPTX_CUDA(cudaMalloc(&g_cache.rec, bytes));
+    g_cache.rec_bytes = bytes;
+  }
+  auto* base = static_cast<unsigned char*>(g_cache.rec);
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    unsigned char* p = base + off;
+    off += (b + 255) & ~size_t(255);
+    return p;
+  };
+  d.fate = take(cap);
+  d.n_boundary = reinterpret_cast<uint32_t*>(take(cap * 4));
+  d.n_scatter = reinterpret_cast<uint32_t*>(take(cap * 4));
+  d.t = reinterpret_cast<float*>(take(cap * 4));
+  d.x = reinterpret_cast<float*>(take(cap * 4));
+  d.y = reinterpret_cast<float*>(take(cap * 4));
+  d.z = reinterpret_cast<float*>(take(cap * 4));
+  d.path = reinterpret_cast<float*>(take(cap * 4));
+  return OPTX_OK;
+}
+
+int cache_tally(size_t len) {
+  if (g_cache.tally_bytes < len * 8) {
+    if (g_cache.tally) cudaFree(g_cache.tally);
+    g_cache.tally = nullptr;
+    g_cache.tally_bytes = 0;
+    OPTX_CUDA(cudaMalloc(&g_cache.tally, len * 8));
+    g_cache.tally_bytes = len * 8;
+  }
+  return OPTX_OK;
+}
+
+int copy_records_d2h(const optx_records* out, uint64_t offset, const DevRecords& d, uint64_t m) {
+  OPTX_CUDA(cudaMemcpy(out->fate + offset, d.fate, m, cudaMemcpyDeviceToHost));
+  OPTX_CUDA(cudaMemcpy(out->n_boundary + offset, d.n_boundary, m * 4, cudaMemcpyDeviceToHost));
+  OPTX_CUDA(cudaMemcpy(out->n_scatter + offset, d.n_scatter, m * 4, cudaMemcpyDeviceToHost));
+  OPTX_CUDA(cudaMemcpy(out->t + offset, d.t, m * 4, cudaMemcpyDeviceToHost));
+  OPTX_CUDA(cudaMemcpy(out->x + offset, d.x, m * 4, cudaMemcpyDeviceToHost));
+  OPTX_CUDA(cudaMemcpy(out->y + offset, d.y, m * 4, cudaMemcpyDeviceToHost));
+  OPTX_CUDA(cudaMemcpy(out->z + offset, d.z, m * 4, cudaMemcpyDeviceToHost));
+  OPTX_CUDA(cudaMemcpy(out->path + offset, d.path, m * 4, cudaMemcpyDeviceToHost));
+  return OPTX_OK;
+}
+
+int check_records(const optx_records* r) {
+  if (r == nullptr || r->fate == nullptr || r->n_boundary == nullptr || r->n_scatter == nullptr ||
+      r->t == nullptr || r->x == nullptr || r->y == nullptr || r->z == nullptr || r->path == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "records: every array must be non-NULL");
+  return OPTX_OK;
+}
+
+DevRecords to_dev(const optx_records* r) {
+  return {r->fate, r->n_boundary, r->n_scatter, r->t, r->x, r->y, r->z, r->path};
+}
+
+}  // namespace
+
+// =============================================================================
+// Wavefront engine object.
+struct optx_engine {
+  optx_wave_config cfg{};
+  optx_tally_config tcfg{};
+  TallyDev tdev{};
+  uint32_t max_events = 0;
+  uint64_t max_photons = 0;
+  int n_sm = 0;
+  size_t smem_tally = 0, smem_tally_batch = 0, smem_adj = 0;
+  uint32_t qcap = 0;
+  // device memory
+  WaveArgs* d_args = nullptr;
+  WaveCtrl* d_ctrl = nullptr;
+  DevParams* d_params = nullptr;
+  unsigned long long* d_offsets = nullptr;
+  float4* d_qa = nullptr;
+  float4* d_qb = nullptr;
+  unsigned long long* d_tally = nullptr;
+  double* d_grad = nullptr;
+  double* d_wbin = nullptr;
+  // current batch
+  uint32_t n_events = 0;
+  uint64_t total = 0;
+  uint64_t first_id = 0;
+  DevParams P0{};
+  std::vector<DevParams> h_params;
+  std::vector<unsigned long long> h_offsets;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool timed = false;
+  struct Graph {
+    int mode;
+    bool batch;
+    int grid, block;
+    size_t smem;
+    DevParams P0;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    cudaGraphConditionalHandle handle;
+  };
+  std::vector<Graph> graphs;
+};
+
+namespace {
+
+size_t wave_smem(const optx_engine* e, int mode, bool batch) {
+  if (mode == kModeTally && !batch) return static_cast<size_t>(e->tdev.len - 7u) * 4u;
+  if (mode == kModeAdjoint) return static_cast<size_t>(e->tdev.time_bins + 1u) * 8u;
+  return 0;
+}
+
+int engine_grid(optx_engine* e, int mode, bool batch, int& grid) {
+  const size_t smem = wave_smem(e, mode, batch);
+  const int math = e->cfg.math;
+  if (smem > 48 * 1024) OPTX_CUDA(DISPATCH(math, wave_set_smem, mode, batch, smem));
+  int bps = DISPATCH(math, wave_blocks_per_sm, mode, batch, e->cfg.block_size, smem);
+  if (bps <= 0) return fail(OPTX_ERR_RUNTIME, "wavefront kernel cannot be resident with this block size / tally");
+  if (e->cfg.blocks_per_sm > 0) bps = std::min(bps, e->cfg.blocks_per_sm);
+  grid = bps * e->n_sm;
+  return OPTX_OK;
+}
+
+// Writes the WaveArgs for a run (async on stream).
+int engine_upload_args(optx_engine* e, int mode, bool batch, int grid, cudaGraphConditionalHandle h,
+                       const DevRecords* rec, const double* w_bin, double w_det,
+                       const double* theta_inv, uint32_t score_mask, cudaStream_t st) {
+  WaveArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.params = e->d_params;
+  a.offsets = e->d_offsets;
+  a.n_events = e->n_events;
+  a.threshold = e->cfg.threshold;
+  a.cadence = e->cfg.cadence;
+  a.qcap = e->qcap;
+  a.total = e->total;
+  a.first_id = e->first_id;
+  a.wave_quota = e->cfg.wave_quota ? e->cfg.wave_quota : (1ull << 31);
+  if (a.wave_quota > (1ull << 30)) a.wave_quota = 1ull << 30;
+  a.qa = e->d_qa;
+  a.qb = e->d_qb;
+  a.tally = (mode == kModeTally) ? e->d_tally : nullptr;
+  a.tc = e->tdev;
+  if (rec) a.rec = *rec;
+  a.w_bin = w_bin;
+  a.w_det = w_det;
+  if (theta_inv) {
+    a.inv_la = theta_inv[0];
+    a.inv_la2 = theta_inv[1];
+    a.inv_ls = theta_inv[2];
+    a.inv_ls2 = theta_inv[3];
+    a.inv_r = theta_inv[4];
+    a.inv_tau = theta_inv[5];
+    a.inv_tau2 = theta_inv[6];
+  }
+  a.score_mask = score_mask;
+  a.grad = (mode == kModeAdjoint) ? e->d_grad : nullptr;
+  a.graph_handle = h;
+  // Watchdog: no warp can iterate more than (photons + queue) x (max_steps + 2) times.
+  uint32_t max_steps = 0;
+  for (const DevParams& p : e->h_params) max_steps = std::max(max_steps, p.max_steps);
+  a.iter_cap = (static_cast<unsigned long long>(e->total) + e->qcap + 64ull) *
+                   (static_cast<unsigned long long>(max_steps) + 2ull) + 4096ull;
+  (void)grid;
+  (void)batch;
+  OPTX_CUDA(cudaMemcpyAsync(e->d_args, &a, sizeof(a), cudaMemcpyHostToDevice, st));
+  return OPTX_OK;
+}
+
+int engine_graph(optx_engine* e, int mode, bool batch, int grid, optx_engine::Graph** out) {
+  const size_t smem = wave_smem(e, mode, batch);
+  const DevParams P0 = batch ? DevParams{} : e->P0;
+  for (auto& g : e->graphs) {
+    if (g.mode == mode && g.batch == batch && g.grid == grid && g.block == e->cfg.block_size &&
+        g.smem == smem && std::memcmp(&g.P0, &P0, sizeof(P0)) == 0) {
+      *out = &g;
+      return OPTX_OK;
+    }
+  }
+  optx_engine::Graph g{};
+  g.mode = mode;
+  g.batch = batch;
+  g.grid = grid;
+  g.block = e->cfg.block_size;
+  g.smem = smem;
+  g.P0 = P0;
+  const int math = e->cfg.math;
+  OPTX_CUDA(cudaGraphCreate(&g.graph, 0));
+  OPTX_CUDA(cudaGraphConditionalHandleCreate(&g.handle, g.graph, 1u, cudaGraphCondAssignDefault));
+
+  // prep: reset the control block, zero the tallies
+  cudaKernelNodeParams kp{};
+  WaveArgs* a_ptr = e->d_args;
+  WaveCtrl* c_ptr = e->d_ctrl;
+  void* prep_args[] = {&a_ptr, &c_ptr};
+  kp.func = const_cast<void*>(DISPATCH(math, wave_prep_fn));
+  kp.gridDim = dim3(std::max(1, std::min(grid, 4 * e->n_sm)));
+  kp.blockDim = dim3(256);
+  kp.sharedMemBytes = 0;
+  kp.kernelParams = prep_args;
+  cudaGraphNode_t n_prep;
+  OPTX_CUDA(cudaGraphAddKernelNode(&n_prep, g.graph, nullptr, 0, &kp));
+
+  // while (active) { wave }
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = g.handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t n_while;
+  OPTX_CUDA(cudaGraphAddNode(&n_while, g.graph, &n_prep, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+
+  DevParams p_copy = P0;
+  void* wave_args[] = {&p_copy, &a_ptr, &c_ptr};
+  cudaKernelNodeParams wp{};
+  wp.func = const_cast<void*>(DISPATCH(math, wave_kernel_fn, mode, batch));
+  wp.gridDim = dim3(grid);
+  wp.blockDim = dim3(e->cfg.block_size);
+  wp.sharedMemBytes = static_cast<unsigned>(smem);
+  wp.kernelParams = wave_args;
+  cudaGraphNode_t n_wave;
+  OPTX_CUDA(cudaGraphAddKernelNode(&n_wave, body, nullptr, 0, &wp));
+  OPTX_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+  e->graphs.push_back(g);
+  *out = &e->graphs.back();
+  return OPTX_OK;
+}
+
+// One complete run of the uploaded batch in `mode` (async on st).
+int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_bin, double w_det,
+               const double* theta_inv, uint32_t score_mask, cudaStream_t st) {
+  if (e->n_events == 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "no events uploaded");
+  const bool batch = e->n_events > 1;
+  int grid = 0;
+  OPTX_TRY(engine_grid(e, mode, batch, grid));
+  const size_t smem = wave_smem(e, mode, batch);
+  const int math = e->cfg.math;
+  if (e->cfg.use_graph >= 0) {
+    optx_engine::Graph* g = nullptr;
+    OPTX_TRY(engine_graph(e, mode, batch, grid, &g));
+    OPTX_TRY(engine_upload_args(e, mode, batch, grid, g->handle, rec, w_bin, w_det, theta_inv,
+                                score_mask, st));
+    OPTX_CUDA(cudaEventRecord(e->ev0, st));
+    OPTX_CUDA(cudaGraphLaunch(g->exec, st));
+    OPTX_CUDA(cudaEventRecord(e->ev1, st));
+  } else {
+    OPTX_TRY(engine_upload_args(e, mode, batch, grid, 0ull, rec, w_bin, w_det, theta_inv,
+                                score_mask, st));
+    OPTX_CUDA(cudaEventRecord(e->ev0, st));
+    OPTX_CUDA(DISPATCH(math, launch_wave_prep, e->d_args, e->d_ctrl,
+                       std::max(1, std::min(grid, 4 * e->n_sm)), 256, st));
+    const DevParams P0 = batch ? DevParams{} : e->P0;
+    for (uint64_t w = 0;; ++w) {
+      OPTX_CUDA(DISPATCH(math, launch_wave, mode, batch, P0, e->d_args, e->d_ctrl, grid,
+                         e->cfg.block_size, smem, st));
+      unsigned active = 0;
+      OPTX_CUDA(cudaMemcpyAsync(&active, &e->d_ctrl->active, sizeof(active),
+                                cudaMemcpyDeviceToHost, st));
+      OPTX_CUDA(cudaStreamSynchronize(st));
+      if (!active) break;
+      if (w > (1ull << 24)) return fail(OPTX_ERR_WATCHDOG, "wavefront did not finish");
+    }
+    OPTX_CUDA(cudaEventRecord(e->ev1, st));
+  }
+  e->timed = true;
+  return OPTX_OK;
+}
+
+int engine_check_ctrl(optx_engine* e, WaveCtrl& c, cudaStream_t st) {
+  OPTX_CUDA(cudaMemcpyAsync(&c, e->d_ctrl, sizeof(c), cudaMemcpyDeviceToHost, st));
+  OPTX_CUDA(cudaStreamSynchronize(st));
+  if (c.error & kErrQueue) return fail(OPTX_ERR_CAPACITY, "wavefront state queue overflow");
+  if (c.error & kErrWatchdog) return fail(OPTX_ERR_WATCHDOG, "wavefront iteration cap reached");
+  return OPTX_OK;
+}
+
+}  // namespace
+
+// =============================================================================
+extern "C" {
+
+int optx_abi_version(void) { return OPTX_ABI_VERSION; }
+
+int optx_gpu_available(void) {
+  int count = 0;
+  const bool ok = cudaGetDeviceCount(&count) == cudaSuccess && count > 0;
+  if (!ok) cudaGetLastError();
+  return ok ? 1 : 0;
+}
+
+int optx_gpu_device_name(char* buf, size_t len) {
+  if (buf == nullptr || len == 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "buffer must not be empty");
+  int dev = 0;
+  cudaDeviceProp prop{};
+  std::string s = "none";
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+    s = std::string(prop.name) + " (sm_" + std::to_string(prop.major) + std::to_string(prop.minor) +
+        ", " + std::to_string(prop.multiProcessorCount) + " SMs)";
+  } else {
+    cudaGetLastError();
+  }
+  std::snprintf(buf, len, "%s", s.c_str());
+  return OPTX_OK;
+}
+
+const char* optx_last_error(void) { return g_err.c_str(); }
+
+int optx_release_cache(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_cache.rec) cudaFree(g_cache.rec);
+  if (g_cache.tally) cudaFree(g_cache.tally);
+  if (g_cache.e0) cudaEventDestroy(g_cache.e0);
+  if (g_cache.e1) cudaEventDestroy(g_cache.e1);
+  g_cache = Cache{};
+  return OPTX_OK;
+}
+
+int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
+                     const optx_records* out, int block_size, uint64_t first_id, uint64_t chunk,
+                     int math, optx_timing* timing) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  OPTX_TRY(check_params(p, faces));
+  OPTX_TRY(check_block(block_size));
+  OPTX_TRY(check_math(math));
+  if (n > 0) OPTX_TRY(check_records(out));
+  OPTX_TRY(ensure_device());
+  OPTX_TRY(cache_events());
+  optx_timing tm{};
+  const auto t0 = std::chrono::steady_clock::now();
+  const DevParams P = make_dev_params(*p, faces);
+  const uint64_t cap = std::max<uint64_t>(1, std::min<uint64_t>(n, chunk ? chunk : (uint64_t{1} << 24)));
+  const auto ta = std::chrono::steady_clock::now();
+  DevRecords d{};
+  OPTX_TRY(cache_records(cap, d));
+  tm.alloc_ms = ms_since(ta);
+  for (uint64_t done = 0; done < n; done += cap) {
+    const uint64_t m = std::min(cap, n - done);
+    OPTX_CUDA(cudaEventRecord(g_cache.e0, 0));
+    OPTX_CUDA(DISPATCH(math, launch_history_records, P, first_id + done, m, d, block_size, nullptr));
+    OPTX_CUDA(cudaEventRecord(g_cache.e1, 0));
+    OPTX_CUDA(cudaEventSynchronize(g_cache.e1));
+    float ms = 0.f;
+    OPTX_CUDA(cudaEventElapsedTime(&ms, g_cache.e0, g_cache.e1));
+    tm.kernel_ms += ms;
+    const auto tc = std::chrono::steady_clock::now();
+    OPTX_TRY(copy_records_d2h(out, done, d, m));
+    tm.d2h_ms += ms_since(tc);
+  }
+  tm.total_ms = ms_since(t0);
+  if (timing) *timing = tm;
+  return OPTX_OK;
+}
+
+int optx_run_tally(const optx_params* p, const optx_faces* faces, const optx_tally_config* c,
+                   uint64_t n, uint64_t* tally_out, int block_size, uint64_t first_id, int math,
+                   optx_timing* timing) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  OPTX_TRY(check_params(p, faces));
+  OPTX_TRY(check_block(block_size));
+  OPTX_TRY(check_math(math));
+  TallyDev td{};
+  OPTX_TRY(make_tally_dev(c, td));
+  if (tally_out == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "tally_out must not be NULL");
+  OPTX_TRY(ensure_device());
+  OPTX_TRY(cache_events());
+  optx_timing tm{};
+  const auto t0 = std::chrono::steady_clock::now();
+  const DevParams P = make_dev_params(*p, faces);
+  const size_t smem = static_cast<size_t>(td.len - 7u) * 4u;
+  int dev = 0, max_smem = 0;
+  OPTX_CUDA(cudaGetDevice(&dev));
+  OPTX_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (smem > static_cast<size_t>(max_smem))
+    return fail(OPTX_ERR_RUNTIME, "tally histograms need " + std::to_string(smem) +
+                                      " bytes of shared memory; reduce xy_bins / time_bins");
+  const int bps = DISPATCH(math, history_tally_blocks_per_sm, block_size, smem);
+  const uint64_t needed = (n + block_size - 1) / block_size;
+  const int grid = static_cast<int>(std::max<uint64_t>(
+      1, std::min<uint64_t>(needed, static_cast<uint64_t>(std::max(bps, 1)) * num_sms())));
+  if (n / grid >= 0xffffffffull)
+    return fail(OPTX_ERR_RUNTIME, "too many photons for one tally launch; split the run");
+  const auto ta = std::chrono::steady_clock::now();
+  OPTX_TRY(cache_tally(td.len));
+  OPTX_CUDA(cudaMemset(g_cache.tally, 0, td.len * 8ull));
+  tm.alloc_ms = ms_since(ta);
+  OPTX_CUDA(cudaEventRecord(g_cache.e0, 0));
+  if (n > 0) OPTX_CUDA(DISPATCH(math, launch_history_tally, P, td, first_id, n, g_cache.tally, block_size, grid, nullptr));
+  OPTX_CUDA(cudaEventRecord(g_cache.e1, 0));
+  OPTX_CUDA(cudaEventSynchronize(g_cache.e1));
+  float ms = 0.f;
+  OPTX_CUDA(cudaEventElapsedTime(&ms, g_cache.e0, g_cache.e1));
+  tm.kernel_ms = ms;
+  const auto tc = std::chrono::steady_clock::now();
+  OPTX_CUDA(cudaMemcpy(tally_out, g_cache.tally, td.len * 8ull, cudaMemcpyDeviceToHost));
+  tm.d2h_ms = ms_since(tc);
+  tm.total_ms = ms_since(t0);
+  if (timing) *timing = tm;
+  return OPTX_OK;
+}
+
+int optx_records_device(const optx_params* p, const optx_faces* faces, uint64_t n,
+                        uint64_t first_id, const optx_records* dev_out, int block_size, int math,
+                        void* stream) {
+  OPTX_TRY(check_params(p, faces));
+  OPTX_TRY(check_block(block_size));
+  OPTX_TRY(check_math(math));
+  if (n > 0) OPTX_TRY(check_records(dev_out));
+  OPTX_TRY(ensure_device());
+  const DevParams P = make_dev_params(*p, faces);
+  const DevRecords d = to_dev(dev_out);
+  // The grid is 32-bit: launch in pieces of at most 2^31 photons.
+  for (uint64_t done = 0; done < n;) {
+    const uint64_t m = std::min<uint64_t>(n - done, 1ull << 31);
+    DevRecords dd = d;
+    dd.fate += done;
+    dd.n_boundary += done;
+    dd.n_scatter += done;
+    dd.t += done;
+    dd.x += done;
+    dd.y += done;
+    dd.z += done;
+    dd.path += done;
+    OPTX_CUDA(DISPATCH(math, launch_history_records, P, first_id + done, m, dd, block_size,
+                       static_cast<cudaStream_t>(stream)));
+    done += m;
+  }
+  return OPTX_OK;
+}
+
+int optx_tally_device(const optx_params* p, const optx_faces* faces, const optx_tally_config* c,
+                      uint64_t n, uint64_t first_id, uint64_t* dev_tally, int block_size, int math,
+                      void* stream) {
+  OPTX_TRY(check_params(p, faces));
+  OPTX_TRY(check_block(block_size));
+  OPTX_TRY(check_math(math));
+  TallyDev td{};
+  OPTX_TRY(make_tally_dev(c, td));
+  if (dev_tally == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "dev_tally must not be NULL");
+  OPTX_TRY(ensure_device());
+  const size_t smem = static_cast<size_t>(td.len - 7u) * 4u;
+  int dev = 0, max_smem = 0;
+  OPTX_CUDA(cudaGetDevice(&dev));
+  OPTX_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (smem > static_cast<size_t>(max_smem))
+    return fail(OPTX_ERR_RUNTIME, "tally histograms need " + std::to_string(smem) +
+                                      " bytes of shared memory; reduce xy_bins / time_bins");
+  if (n == 0) return OPTX_OK;
+  const DevParams P = make_dev_params(*p, faces);
+  const int bps = DISPATCH(math, history_tally_blocks_per_sm, block_size, smem);
+  const uint64_t needed = (n + block_size - 1) / block_size;
+  const int grid = static_cast<int>(std::max<uint64_t>(
+      1, std::min<uint64_t>(needed, static_cast<uint64_t>(std::max(bps, 1)) * num_sms())));
+  if (n / grid >= 0xffffffffull)
+    return fail(OPTX_ERR_RUNTIME, "too many photons for one tally launch; split the run");
+  OPTX_CUDA(DISPATCH(math, launch_history_tally, P, td, first_id, n,
+                     reinterpret_cast<unsigned long long*>(dev_tally), block_size, grid,
+                     static_cast<cudaStream_t>(stream)));
+  return OPTX_OK;
+}
+
+// ---- wavefront engine ---------------------------------------------------------
+
+int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t max_photons,
+                       const optx_wave_config* cfg, optx_engine** out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (out == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "out must not be NULL");
+  *out = nullptr;
+  if (max_events == 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "max_events must be >= 1");
+  if (max_photons == 0 || max_photons > 0xffffffffull)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "max_photons must be in [1, 2^32 - 1] per run");
+  TallyDev td{};
+  OPTX_TRY(make_tally_dev(c, td));
+  optx_wave_config k{};
+  if (cfg) k = *cfg;
+  if (k.block_size == 0) k.block_size = 256;
+  OPTX_TRY(check_block(k.block_size));
+  if (k.threshold == 0) k.threshold = 24;
+  if (k.threshold > 32) return fail(OPTX_ERR_INVALID_ARGUMENT, "threshold must be 1..32");
+  if (k.use_graph == 0) k.use_graph = 1;
+  OPTX_TRY(check_math(k.math));
+  OPTX_TRY(ensure_device());
+  auto* e = new optx_engine();
+  e->cfg = k;
+  e->tcfg = *c;
+  e->tdev = td;
+  e->max_events = max_events;
+  e->max_photons = max_photons;
+  e->n_sm = num_sms();
+  auto cleanup = [&](int rc) {
+    optx_engine_destroy(e);
+    return rc;
+  };
+  int grid_max = 0;
+  for (int mode = 0; mode < 3; ++mode) {
+    for (int b = 0; b < 2; ++b) {
+      int g = 0;
+      const int rc = engine_grid(e, mode, b == 1, g);
+      if (rc != OPTX_OK && mode == kModeTally) return cleanup(rc);
+      grid_max = std::max(grid_max, g);
+    }
+  }
+  const uint64_t lanes = static_cast<uint64_t>(grid_max) * k.block_size;
+  uint64_t qcap = lanes;
+  if (k.cadence != 0) qcap = std::max<uint64_t>(lanes, std::min<uint64_t>(max_photons, 1ull << 23));
+  qcap = (qcap + 31) & ~uint64_t(31);
+  e->qcap = static_cast<uint32_t>(qcap);
+  auto alloc = [&](void** p, size_t bytes) -> int {
+    const cudaError_t err = cudaMalloc(p, bytes);
+    if (err != cudaSuccess) {
+      cudaGetLastError();
+      return fail(OPTX_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
+    }
+    return OPTX_OK;
+  };
+  int rc = OPTX_OK;
+  if ((rc = alloc(reinterpret_cast<void**>(&e->d_args), sizeof(WaveArgs))) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_ctrl), sizeof(WaveCtrl))) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_params), sizeof(DevParams) * max_events)) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_offsets), 8ull * (max_events + 1ull))) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_qa), qcap * 64ull)) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_qb), qcap * 64ull)) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_tally), 8ull * td.len * max_events)) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_grad), 8ull * 4)) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_wbin), 8ull * (td.time_bins + 1ull))))
+    return cleanup(rc);
+  if (cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess)
+    return cleanup(fail(OPTX_ERR_CUDA, "cudaEventCreate failed"));
+  *out = e;
+  return OPTX_OK;
+}
+
+int optx_engine_destroy(optx_engine* e) {
+  if (e == nullptr) return OPTX_OK;
+  for (auto& g : e->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+  }
+  cudaFree(e->d_args);
+  cudaFree(e->d_ctrl);
+  cudaFree(e->d_params);
+  cudaFree(e->d_offsets);
+  cudaFree(e->d_qa);
+  cudaFree(e->d_qb);
+  cudaFree(e->d_tally);
+  cudaFree(e->d_grad);
+  cudaFree(e->d_wbin);
+  if (e->ev0) cudaEventDestroy(e->ev0);
+  if (e->ev1) cudaEventDestroy(e->ev1);
+  delete e;
+  return OPTX_OK;
+}
+
+int optx_engine_set_events(optx_engine* e, const optx_params* events, const optx_faces* faces,
+                           const uint64_t* counts, uint32_t n_events, uint64_t first_id,
+                           void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "engine must not be NULL");
+  if (n_events == 0 || n_events > e->max_events)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "n_events must be in [1, max_events]");
+  if (events == nullptr || counts == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "events and counts must not be NULL");
+  e->h_params.resize(n_events);
+  e->h_offsets.resize(n_events + 1ull);
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < n_events; ++i) {
+    OPTX_TRY(check_params(&events[i], faces ? &faces[i] : nullptr));
+    e->h_params[i] = make_dev_params(events[i], faces ? &faces[i] : nullptr);
+    e->h_offsets[i] = total;
+    total += counts[i];
+    if (total > e->max_photons)
+      return fail(OPTX_ERR_INVALID_ARGUMENT, "batch exceeds the engine's max_photons");
+  }
+  e->h_offsets[n_events] = total;
+  e->n_events = n_events;
+  e->total = total;
+  e->first_id = first_id;
+  e->P0 = e->h_params[0];
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  OPTX_CUDA(cudaMemcpyAsync(e->d_params, e->h_params.data(), sizeof(DevParams) * n_events,
+                            cudaMemcpyHostToDevice, st));
+  OPTX_CUDA(cudaMemcpyAsync(e->d_offsets, e->h_offsets.data(), 8ull * (n_events + 1ull),
+                            cudaMemcpyHostToDevice, st));
+  return OPTX_OK;
+}
+
+int optx_engine_run_tally(optx_engine* e, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "engine must not be NULL");
+  return engine_run(e, kModeTally, nullptr, nullptr, 0.0, nullptr, 0u,
+                    static_cast<cudaStream_t>(stream));
+}
+
+int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "engine must not be NULL");
+  OPTX_TRY(check_records(dev_out));
+  const DevRecords d = to_dev(dev_out);
+  return engine_run(e, kModeRecords, &d, nullptr, 0.0, nullptr, 0u,
+                    static_cast<cudaStream_t>(stream));
+}
+
+int optx_engine_tally_ptr(optx_engine* e, uint64_t** dev_ptr, uint64_t* len_per_event) {
+  if (e == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "engine must not be NULL");
+  if (dev_ptr) *dev_ptr = reinterpret_cast<uint64_t*>(e->d_tally);
+  if (len_per_event) *len_per_event = e->tdev.len;
+  return OPTX_OK;
+}
+
+int optx_engine_get_tallies(optx_engine* e, uint64_t* host_out, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr || host_out == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "engine and host_out must not be NULL");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WaveCtrl c{};
+  OPTX_TRY(engine_check_ctrl(e, c, st));
+  OPTX_CUDA(cudaMemcpyAsync(host_out, e->d_tally, 8ull * e->tdev.len * e->n_events,
+                            cudaMemcpyDeviceToHost, st));
+  OPTX_CUDA(cudaStreamSynchronize(st));
+  return OPTX_OK;
+}
+
+int optx_engine_stats(optx_engine* e, optx_event_stats* stats, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr || stats == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "engine and stats must not be NULL");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WaveCtrl c{};
+  OPTX_TRY(engine_check_ctrl(e, c, st));
+  stats->launches = c.wave;
+  stats->useful_lane_steps = c.useful;
+  stats->issued_lane_steps = c.issued;
+  stats->spills = c.spills;
+  float ms = 0.f;
+  if (e->timed) OPTX_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+  stats->kernels_ms = ms;
+  return OPTX_OK;
+}
+
+int optx_run_batch(optx_engine* e, const optx_params* events, const optx_faces* faces,
+                   const uint64_t* counts, uint32_t n_events, uint64_t first_id,
+                   uint64_t* host_tallies, optx_event_stats* stats, optx_timing* timing) {
+  if (e == nullptr || host_tallies == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "engine and host_tallies must not be NULL");
+  optx_timing tm{};
+  const auto t0 = std::chrono::steady_clock::now();
+  OPTX_TRY(optx_engine_set_events(e, events, faces, counts, n_events, first_id, nullptr));
+  OPTX_TRY(optx_engine_run_tally(e, nullptr));
+  OPTX_TRY(optx_engine_get_tallies(e, host_tallies, nullptr));
+  tm.total_ms = ms_since(t0);
+  optx_event_stats s{};
+  OPTX_TRY(optx_engine_stats(e, &s, nullptr));
+  tm.kernel_ms = s.kernels_ms;
+  if (stats) *stats = s;
+  if (timing) *timing = tm;
+  return OPTX_OK;
+}
+
+int optx_run_records_event(const optx_params* p, const optx_faces* faces, uint64_t n,
+                           const optx_records* out, uint32_t steps_per_launch, int block_size,
+                           uint64_t first_id, uint64_t chunk, int math, optx_event_stats* stats,
+                           optx_timing* timing) {
+  OPTX_TRY(check_params(p, faces));
+  OPTX_TRY(check_block(block_size));
+  if (steps_per_launch == 0)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "event-based backend: steps_per_launch must be >= 1");
+  OPTX_TRY(check_math(math));
+  if (n > 0) OPTX_TRY(check_records(out));
+  OPTX_TRY(ensure_device());
+  const auto t0 = std::chrono::steady_clock::now();
+  const uint64_t cap = std::max<uint64_t>(1, std::min<uint64_t>({n, chunk ? chunk : (uint64_t{1} << 24), uint64_t{1} << 31}));
+  optx_tally_config tc{1u, 1.0f, 1u};
+  optx_wave_config cfg{};
+  cfg.block_size = block_size;
+  cfg.threshold = 32;
+  cfg.cadence = steps_per_launch >= p->max_steps ? 0u : steps_per_launch;
+  cfg.use_graph = 1;
+  cfg.math = math;
+  optx_engine* e = nullptr;
+  OPTX_TRY(optx_engine_create(&tc, 1, cap, &cfg, &e));
+  optx_timing tm{};
+  optx_event_stats st{};
+  int rc = OPTX_OK;
+  {
+    std::unique_lock<std::mutex> lk(g_mu);
+    DevRecords d{};
+    rc = cache_records(cap, d);
+    lk.unlock();
+    for (uint64_t done = 0; rc == OPTX_OK && done < n; done += cap) {
+      const uint64_t m = std::min(cap, n - done);
+      const uint64_t cnt = m;
+      if ((rc = optx_engine_set_events(e, p, faces, &cnt, 1, first_id + done, nullptr)) != OPTX_OK) break;
+      const optx_records dr{d.fate, d.n_boundary, d.n_scatter, d.t, d.x, d.y, d.z, d.path};
+      if ((rc = optx_engine_run_records(e, &dr, nullptr)) != OPTX_OK) break;
+      optx_event_stats s{};
+      if ((rc = optx_engine_stats(e, &s, nullptr)) != OPTX_OK) break;
+      st.launches += s.launches;
+      st.useful_lane_steps += s.useful_lane_steps;
+      st.issued_lane_steps += s.issued_lane_steps;
+      st.spills += s.spills;
+      st.kernels_ms += s.kernels_ms;
+      const auto tcp = std::chrono::steady_clock::now();
+      lk.lock();
+      rc = copy_records_d2h(out, done, d, m);
+      lk.unlock();
+      tm.d2h_ms += ms_since(tcp);
+    }
+  }
+  optx_engine_destroy(e);
+  if (rc != OPTX_OK) return rc;
+  tm.kernel_ms = st.kernels_ms;
+  tm.total_ms = ms_since(t0);
+  if (stats) *stats = st;
+  if (timing) *timing = tm;
+  return OPTX_OK;
+}
+
+}  // extern "C"

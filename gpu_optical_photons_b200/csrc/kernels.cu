@@ -1,0 +1,563 @@
+// kernels.cu - photon transport kernels for sm_100a.
+//
+// Compiled twice by the build: OPTX_NS=fast (CUDA libm, FMA contraction) and
+// OPTX_NS=exact (portable math, -fmad=false). Kernels:
+//
+//  * history_records_kernel / history_tally_kernel: one thread per photon for
+//    its whole history, the drop-in for the reference's transport_records_kernel
+//    and transport_tally_kernel (src/gpu/gpu_backend.cu:47-100 of the reference).
+//    The tally keeps fate counts and step sums in registers (no atomics) and the
+//    time / hit-map histograms in block-private shared memory, flushed once per
+//    block with 64-bit global atomics: integer sums, so the result does not depend
+//    on the schedule (the property of gpu_backend.cu:68-100 and test_gpu.cpp:122-146).
+//
+//  * wave_kernel: the wavefront engine, the B200 form of the reference's
+//    event_step_kernel (src/gpu/gpu_event.cu:125-170). A persistent grid of warps
+//    keeps one photon per lane in registers. When fewer than `threshold` lanes of
+//    a warp are alive, the warp takes the next work items with one atomic
+//    (warp-aggregated) and the idle lanes load a survivor of the previous wave
+//    from the state queue or emit a fresh photon, so warps stay full instead of
+//    waiting for their longest history. When the wave's items are used up, or a
+//    photon has made `cadence` steps in this wave, the warp spills its live
+//    photons: ballot + popc give each one a slot after a single atomicAdd, and the
+//    state is written as 4 x 128-bit stores into an AoSoA queue tile (32 photons x
+//    64 B). The next wave (the next iteration of a CUDA-graph while loop, or the
+//    next host launch) reads them back with 4 x 128-bit coalesced loads. The
+//    last block to finish a wave sets up the next one (counters only; no block
+//    ever waits for another). Photons may belong to different events (batched
+//    mode): each lane then reads its event's 112-byte parameter record with
+//    7 x 128-bit loads per step, and tallies go to that event's slice.
+//    Records depend only on (seed, photon id), so they equal the history
+//    kernel's bit for bit for any block size, threshold, cadence or wave size.
+#include <cuda_runtime.h>
+
+#include "optx_device.cuh"
+#include "optx_engine.hpp"
+
+#ifndef OPTX_NS
+#error "OPTX_NS must be defined (fast or exact)"
+#endif
+
+namespace optx {
+namespace OPTX_NS {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ void store_record(const DevRecords& out, uint64_t i, const Photon& s,
+                                             uint32_t fate) {
+  out.fate[i] = static_cast<uint8_t>(fate);
+  out.n_boundary[i] = s.nb;
+  out.n_scatter[i] = s.ns;
+  out.t[i] = s.t;
+  out.x[i] = s.px;
+  out.y[i] = s.py;
+  out.z[i] = s.pz;
+  out.path[i] = s.path;
+}
+
+// The full history of photon `id` (transport.hpp:151-159).
+template <bool AUX>
+__device__ __forceinline__ uint32_t transport(const DevParams& P, uint64_t id, Photon& s,
+                                              ScoreAux& aux) {
+  Rng r;
+  r.init(id, P.key_lo, P.key_hi, 0u);
+  start_photon<AUX>(P, s, r, aux);
+  uint32_t fate = kMaxSteps;
+  for (uint32_t step = 0; step < P.max_steps; ++step) {
+    if (!step_photon<AUX>(P, s, r, fate, aux)) break;
+  }
+  return fate;
+}
+
+__global__ void history_records_kernel(const DevParams P, uint64_t first_id, uint64_t n,
+                                       DevRecords out) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Photon s;
+  ScoreAux aux{0u, 0.0f};
+  const uint32_t fate = transport<false>(P, first_id + i, s, aux);
+  store_record(out, i, s, fate);
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum_f64(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(kFull, v, off);
+  return v;
+}
+
+// Flat tally layout: [5 fates | time_bins + 1 | xy_bins^2 | sum nb | sum ns].
+__global__ void history_tally_kernel(const DevParams P, const TallyDev tc, uint64_t first_id,
+                                     uint64_t n, unsigned long long* __restrict__ gt) {
+  extern __shared__ uint32_t s_hist[];  // [time_bins + 1 | xy_bins^2]
+  const uint32_t n_bins = tc.len - 7u;
+  for (uint32_t b = threadIdx.x; b < n_bins; b += blockDim.x) s_hist[b] = 0u;
+  __syncthreads();
+
+  uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0;
+  unsigned long long snb = 0, sns = 0;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += stride) {
+    Photon s;
+    ScoreAux aux{0u, 0.0f};
+    const uint32_t fate = transport<false>(P, first_id + i, s, aux);
+    f0 += fate == 0u;
+    f1 += fate == 1u;
+    f2 += fate == 2u;
+    f3 += fate == 3u;
+    f4 += fate == 4u;
+    snb += s.nb;
+    sns += s.ns;
+    if (fate == kDetected) {
+      atomicAdd(&s_hist[time_bin(s.t, tc.tscale, tc.time_bins)], 1u);
+      atomicAdd(&s_hist[tc.time_bins + 1u + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins)], 1u);
+    }
+  }
+  // Fates and sums: warp reductions, one global atomic per warp and counter.
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t r0 = __reduce_add_sync(kFull, f0), r1 = __reduce_add_sync(kFull, f1),
+                 r2 = __reduce_add_sync(kFull, f2), r3 = __reduce_add_sync(kFull, f3),
+                 r4 = __reduce_add_sync(kFull, f4);
+  snb = warp_sum_u64(snb);
+  sns = warp_sum_u64(sns);
+  if (lane == 0) {
+    if (r0) atomicAdd(&gt[0], static_cast<unsigned long long>(r0));
+    if (r1) atomicAdd(&gt[1], static_cast<unsigned long long>(r1));
+    if (r2) atomicAdd(&gt[2], static_cast<unsigned long long>(r2));
+    if (r3) atomicAdd(&gt[3], static_cast<unsigned long long>(r3));
+    if (r4) atomicAdd(&gt[4], static_cast<unsigned long long>(r4));
+    if (snb) atomicAdd(&gt[tc.len - 2u], snb);
+    if (sns) atomicAdd(&gt[tc.len - 1u], sns);
+  }
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < n_bins; b += blockDim.x) {
+    if (s_hist[b] != 0u) atomicAdd(&gt[5u + b], static_cast<unsigned long long>(s_hist[b]));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Wavefront engine.
+
+__device__ __forceinline__ DevParams load_params(const DevParams* p) {
+  DevParams P;
+  const float4* src = reinterpret_cast<const float4*>(p);
+  float4* dst = reinterpret_cast<float4*>(&P);
+#pragma unroll
+  for (int i = 0; i < 7; ++i) dst[i] = __ldg(src + i);
+  return P;
+}
+
+// Largest e with offsets[e] <= g (offsets[0] = 0 <= g < offsets[n_events]).
+__device__ __forceinline__ uint32_t find_event(const unsigned long long* __restrict__ offsets,
+                                               uint32_t n_events, unsigned long long g) {
+  uint32_t lo = 0, hi = n_events;
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(offsets + mid) <= g) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Queue slot -> first float4 of the photon in its 32-photon tile.
+__device__ __forceinline__ size_t qidx(uint32_t slot) {
+  return static_cast<size_t>(slot >> 5) * 128u + (slot & 31u);
+}
+
+__global__ void wave_prep_kernel(const WaveArgs* __restrict__ A, WaveCtrl* __restrict__ ctrl) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long fresh = A->total < A->wave_quota ? A->total : A->wave_quota;
+    if (A->cadence != 0u && fresh > A->qcap) fresh = A->qcap;
+    ctrl->fresh_next = 0ull;
+    ctrl->useful = 0ull;
+    ctrl->issued = 0ull;
+    ctrl->wave = 0u;
+    ctrl->n_in = 0u;
+    ctrl->fresh_count = static_cast<unsigned int>(fresh);
+    ctrl->cursor = 0u;
+    ctrl->n_out = 0u;
+    ctrl->blocks_done = 0u;
+    ctrl->active = fresh > 0ull ? 1u : 0u;
+    ctrl->error = 0u;
+    ctrl->spills = 0u;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 4u && A->grad != nullptr) A->grad[threadIdx.x] = 0.0;
+  if (A->tally != nullptr) {
+    const size_t total = static_cast<size_t>(A->n_events) * A->tc.len;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+      A->tally[i] = 0ull;
+  }
+}
+
+template <int MODE, bool BATCH>
+__global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
+                                                   const WaveArgs* __restrict__ A,
+                                                   WaveCtrl* __restrict__ ctrl) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t* s_hist = reinterpret_cast<uint32_t*>(smem_raw);  // tally, not batched
+  double* s_w = reinterpret_cast<double*>(smem_raw);         // adjoint weights
+  __shared__ double s_red[4][32];
+
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+
+  const uint32_t wave = ctrl->wave;
+  const uint32_t n_in = ctrl->n_in;
+  const uint32_t items = n_in + ctrl->fresh_count;
+  const unsigned long long fresh_next = ctrl->fresh_next;
+  const float4* __restrict__ qin = (wave & 1u) ? A->qb : A->qa;
+  float4* __restrict__ qout = (wave & 1u) ? A->qa : A->qb;
+  const uint32_t T = A->threshold;
+  const uint32_t cadence = A->cadence;
+  const uint32_t qcap = A->qcap;
+  const unsigned long long first_id = A->first_id;
+  const unsigned long long iter_cap = A->iter_cap;
+  const TallyDev tc = A->tc;
+
+  if (MODE == kModeTally && !BATCH) {
+    for (uint32_t b = threadIdx.x; b < tc.len - 7u; b += blockDim.x) s_hist[b] = 0u;
+  }
+  if (MODE == kModeAdjoint) {
+    for (uint32_t b = threadIdx.x; b <= tc.time_bins; b += blockDim.x) s_w[b] = A->w_bin[b];
+  }
+  __syncthreads();
+
+  Photon s{};
+  Rng r{};
+  ScoreAux aux{0u, 0.0f};
+  uint32_t pidx = 0u, ev = 0u;
+  bool alive = false, exhausted = false;
+  uint32_t wsteps = 0u;
+  // Per-lane tallies (flushed at the end; batched: when the lane's event changes).
+  uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0;
+  unsigned long long snb = 0, sns = 0;
+  uint32_t cur_ev = 0xffffffffu;
+  double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
+  unsigned long long useful = 0, issued = 0;
+
+  auto flush_event = [&]() {
+    if (cur_ev == 0xffffffffu) return;
+    unsigned long long* T0 = A->tally + static_cast<size_t>(cur_ev) * tc.len;
+    if (f0) atomicAdd(&T0[0], static_cast<unsigned long long>(f0));
+    if (f1) atomicAdd(&T0[1], static_cast<unsigned long long>(f1));
+    if (f2) atomicAdd(&T0[2], static_cast<unsigned long long>(f2));
+    if (f3) atomicAdd(&T0[3], static_cast<unsigned long long>(f3));
+    if (f4) atomicAdd(&T0[4], static_cast<unsigned long long>(f4));
+    if (snb) atomicAdd(&T0[tc.len - 2u], snb);
+    if (sns) atomicAdd(&T0[tc.len - 1u], sns);
+    f0 = f1 = f2 = f3 = f4 = 0u;
+    snb = sns = 0ull;
+  };
+
+  // Bookkeeping of a finished photon.
+  auto finish = [&](uint32_t fate, const DevParams& P) {
+    if (MODE == kModeRecords) {
+      store_record(A->rec, pidx, s, fate);
+    } else if (MODE == kModeTally) {
+      if (BATCH && ev != cur_ev) {
+        flush_event();
+        cur_ev = ev;
+      }
+      f0 += fate == 0u;
+      f1 += fate == 1u;
+      f2 += fate == 2u;
+      f3 += fate == 3u;
+      f4 += fate == 4u;
+      snb += s.nb;
+      sns += s.ns;
+      if (fate == kDetected) {
+        const uint32_t tb = time_bin(s.t, tc.tscale, tc.time_bins);
+        const uint32_t xb = tc.time_bins + 1u + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins);
+        if (BATCH) {
+          unsigned long long* T0 = A->tally + static_cast<size_t>(ev) * tc.len + 5u;
+          atomicAdd(&T0[tb], 1ull);
+          atomicAdd(&T0[xb], 1ull);
+        } else {
+          atomicAdd(&s_hist[tb], 1u);
+          atomicAdd(&s_hist[xb], 1u);
+        }
+      }
+    } else {  // adjoint: score terms of detected photons (see WaveArgs)
+      if (fate == kDetected) {
+        const double w = s_w[time_bin(s.t, tc.tscale, tc.time_bins)] + A->w_det;
+        if (w != 0.0) {
+          const double path = s.path;
+          const uint32_t m = A->score_mask;
+          if (m & 1u) g0 += w * (path * A->inv_la2);
+          if (m & 2u) g1 += w * (path * A->inv_ls2 - static_cast<double>(s.ns) * A->inv_ls);
+          if (m & 4u) g2 += w * (static_cast<double>(aux.n_refl) * A->inv_r);
+          if (m & 8u) g3 += w * (static_cast<double>(aux.t_emit) * A->inv_tau2 - A->inv_tau);
+        }
+      }
+    }
+  };
+
+  // Warp-collective: spill the lanes with `spill` set into the output queue.
+  auto spill_lanes = [&](bool spill) {
+    const uint32_t smask = __ballot_sync(kFull, spill);
+    if (smask == 0u) return;
+    uint32_t base = 0u;
+    if (lane == 0u) base = atomicAdd(&ctrl->n_out, static_cast<unsigned>(__popc(smask)));
+    base = __shfl_sync(kFull, base, 0);
+    if (spill) {
+      const uint32_t slot = base + static_cast<uint32_t>(__popc(smask & lt));
+      if (slot < qcap) {
+        float4* q = qout + qidx(slot);
+        q[0] = make_float4(s.px, s.py, s.pz, s.t);
+        q[32] = make_float4(s.dx, s.dy, s.dz, s.path);
+        q[64] = make_float4(__uint_as_float(s.nb), __uint_as_float(s.ns),
+                            __uint_as_float(r.draws()), __uint_as_float(pidx));
+        q[96] = make_float4(__uint_as_float(aux.n_refl), aux.t_emit, __uint_as_float(ev), 0.0f);
+      } else {
+        atomicOr(&ctrl->error, kErrQueue);
+      }
+    }
+  };
+
+  for (unsigned long long it = 0;; ++it) {
+    if (it > iter_cap) {
+      if (lane == 0u) atomicOr(&ctrl->error, kErrWatchdog);
+      break;
+    }
+    uint32_t amask = __ballot_sync(kFull, alive);
+    if (static_cast<uint32_t>(__popc(amask)) < T) {
+      if (!exhausted) {
+        const uint32_t need = 32u - static_cast<uint32_t>(__popc(amask));
+        uint32_t base = 0u;
+        if (lane == 0u) base = atomicAdd(&ctrl->cursor, need);
+        base = __shfl_sync(kFull, base, 0);
+        const uint32_t got = base >= items ? 0u : min(need, items - base);
+        exhausted = got < need;
+        const uint32_t rank = static_cast<uint32_t>(__popc(~amask & lt));
+        if (!alive && rank < got) {
+          const uint32_t item = base + rank;
+          if (item < n_in) {
+            // A survivor of the previous wave: 4 x 128-bit loads from its tile.
+            const float4* q = qin + qidx(item);
+            const float4 a = q[0], b = q[32], c = q[64], d = q[96];
+            s.px = a.x; s.py = a.y; s.pz = a.z; s.t = a.w;
+            s.dx = b.x; s.dy = b.y; s.dz = b.z; s.path = b.w;
+            s.nb = __float_as_uint(c.x);
+            s.ns = __float_as_uint(c.y);
+            pidx = __float_as_uint(c.w);
+            aux.n_refl = __float_as_uint(d.x);
+            aux.t_emit = d.y;
+            ev = __float_as_uint(d.z);
+            const DevParams P = BATCH ? load_params(A->params + ev) : P0;
+            r.init(first_id + pidx, P.key_lo, P.key_hi, __float_as_uint(c.z));
+            alive = true;
+          } else {
+            const unsigned long long g = fresh_next + (item - n_in);
+            pidx = static_cast<uint32_t>(g);
+            if (BATCH) ev = find_event(A->offsets, A->n_events, g);
+            const DevParams P = BATCH ? load_params(A->params + ev) : P0;
+            r.init(first_id + g, P.key_lo, P.key_hi, 0u);
+            aux.n_refl = 0u;
+            start_photon<MODE == kModeAdjoint>(P, s, r, aux);
+            alive = P.max_steps > 0u;
+            if (!alive) finish(kMaxSteps, P);
+          }
+          wsteps = 0u;
+        }
+        amask = __ballot_sync(kFull, alive);
+      }
+      if (exhausted) {
+        const uint32_t na = static_cast<uint32_t>(__popc(amask));
+        if (na == 0u) break;
+        if (na < T) {
+          spill_lanes(alive);
+          alive = false;
+          break;
+        }
+      }
+    }
+
+    // One step for every live lane.
+    if (alive) {
+      const DevParams P = BATCH ? load_params(A->params + ev) : P0;
+      uint32_t fate = kMaxSteps;
+      const bool still = step_photon<MODE == kModeAdjoint>(P, s, r, fate, aux);
+      ++wsteps;
+      if (!still) {
+        alive = false;
+        finish(fate, P);
+      } else if (s.nb + s.ns >= P.max_steps) {
+        alive = false;
+        finish(kMaxSteps, P);
+      }
+    }
+    issued += 32u;
+    useful += static_cast<uint32_t>(__popc(amask));
+    if (cadence != 0u) {  // forced compaction after `cadence` steps in this wave
+      const bool sp = alive && wsteps >= cadence;
+      spill_lanes(sp);
+      if (sp) alive = false;
+    }
+  }
+
+  // ---- end of this block's share of the wave: flush --------------------------
+  if (lane == 0u) {
+    atomicAdd(&ctrl->useful, useful);
+    atomicAdd(&ctrl->issued, issued);
+  }
+  if (MODE == kModeTally) {
+    if (BATCH) {
+      flush_event();
+    } else {
+      const uint32_t r0 = __reduce_add_sync(kFull, f0), r1 = __reduce_add_sync(kFull, f1),
+                     r2 = __reduce_add_sync(kFull, f2), r3 = __reduce_add_sync(kFull, f3),
+                     r4 = __reduce_add_sync(kFull, f4);
+      const unsigned long long wnb = warp_sum_u64(snb), wns = warp_sum_u64(sns);
+      unsigned long long* gt = A->tally;
+      if (lane == 0u) {
+        if (r0) atomicAdd(&gt[0], static_cast<unsigned long long>(r0));
+        if (r1) atomicAdd(&gt[1], static_cast<unsigned long long>(r1));
+        if (r2) atomicAdd(&gt[2], static_cast<unsigned long long>(r2));
+        if (r3) atomicAdd(&gt[3], static_cast<unsigned long long>(r3));
+        if (r4) atomicAdd(&gt[4], static_cast<unsigned long long>(r4));
+        if (wnb) atomicAdd(&gt[tc.len - 2u], wnb);
+        if (wns) atomicAdd(&gt[tc.len - 1u], wns);
+      }
+      __syncthreads();
+      for (uint32_t b = threadIdx.x; b < tc.len - 7u; b += blockDim.x) {
+        if (s_hist[b] != 0u) atomicAdd(&gt[5u + b], static_cast<unsigned long long>(s_hist[b]));
+      }
+    }
+  }
+  if (MODE == kModeAdjoint) {
+    g0 = warp_sum_f64(g0);
+    g1 = warp_sum_f64(g1);
+    g2 = warp_sum_f64(g2);
+    g3 = warp_sum_f64(g3);
+    if (lane == 0u) {
+      s_red[0][warp] = g0;
+      s_red[1][warp] = g1;
+      s_red[2][warp] = g2;
+      s_red[3][warp] = g3;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4u) {
+      double acc = 0.0;
+      const uint32_t nw = blockDim.x >> 5;
+      for (uint32_t w = 0; w < nw; ++w) acc += s_red[threadIdx.x][w];
+      if (acc != 0.0) atomicAdd(&A->grad[threadIdx.x], acc);
+    }
+  }
+
+  // ---- the last block to finish sets up the next wave --------------------------
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned done = atomicAdd(&ctrl->blocks_done, 1u);
+    if (done == gridDim.x - 1u) {
+      __threadfence();
+      volatile WaveCtrl* vc = ctrl;
+      const unsigned n_out = vc->n_out;
+      const unsigned long long next = vc->fresh_next + vc->fresh_count;
+      const unsigned long long remaining = A->total - next;
+      unsigned long long fresh = remaining < A->wave_quota ? remaining : A->wave_quota;
+      if (A->cadence != 0u) {
+        const unsigned long long room = qcap > n_out ? qcap - n_out : 0ull;
+        if (fresh > room) fresh = room;
+      }
+      vc->fresh_next = next;
+      vc->n_in = n_out;
+      vc->fresh_count = static_cast<unsigned>(fresh);
+      vc->n_out = 0u;
+      vc->cursor = 0u;
+      vc->blocks_done = 0u;
+      vc->spills = vc->spills + n_out;
+      vc->wave = vc->wave + 1u;
+      const bool more = (n_out + fresh) > 0ull && vc->error == 0u;
+      vc->active = more ? 1u : 0u;
+      __threadfence();
+      if (!more && A->graph_handle != 0ull) cudaGraphSetConditional(A->graph_handle, 0u);
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host launchers.
+
+cudaError_t launch_history_records(const DevParams& P, uint64_t first_id, uint64_t n,
+                                   const DevRecords& out, int block, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const uint64_t grid = (n + block - 1) / block;
+  history_records_kernel<<<static_cast<unsigned>(grid), block, 0, st>>>(P, first_id, n, out);
+  return cudaGetLastError();
+}
+
+int history_tally_blocks_per_sm(int block, size_t smem) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, history_tally_kernel, block, smem) !=
+      cudaSuccess)
+    return 0;
+  return b;
+}
+
+cudaError_t launch_history_tally(const DevParams& P, const TallyDev& tc, uint64_t first_id,
+                                 uint64_t n, unsigned long long* tally, int block, int grid,
+                                 cudaStream_t st) {
+  const size_t smem = static_cast<size_t>(tc.len - 7u) * sizeof(uint32_t);
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(
+        history_tally_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+  }
+  history_tally_kernel<<<grid, block, smem, st>>>(P, tc, first_id, n, tally);
+  return cudaGetLastError();
+}
+
+const void* wave_prep_fn() { return reinterpret_cast<const void*>(&wave_prep_kernel); }
+
+cudaError_t launch_wave_prep(const WaveArgs* A_dev, WaveCtrl* ctrl, int grid, int block,
+                             cudaStream_t st) {
+  wave_prep_kernel<<<grid, block, 0, st>>>(A_dev, ctrl);
+  return cudaGetLastError();
+}
+
+template <int MODE, bool BATCH>
+static const void* kfn() {
+  return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH>);
+}
+
+const void* wave_kernel_fn(int mode, bool batch) {
+  switch (mode) {
+    case kModeTally: return batch ? kfn<kModeTally, true>() : kfn<kModeTally, false>();
+    case kModeRecords: return batch ? kfn<kModeRecords, true>() : kfn<kModeRecords, false>();
+    default: return batch ? kfn<kModeAdjoint, true>() : kfn<kModeAdjoint, false>();
+  }
+}
+
+int wave_blocks_per_sm(int mode, bool batch, int block, size_t smem) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, wave_kernel_fn(mode, batch), block, smem) !=
+      cudaSuccess)
+    return 0;
+  return b;
+}
+
+cudaError_t wave_set_smem(int mode, bool batch, size_t smem) {
+  return cudaFuncSetAttribute(wave_kernel_fn(mode, batch),
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+}
+
+cudaError_t launch_wave(int mode, bool batch, const DevParams& P, const WaveArgs* A_dev,
+                        WaveCtrl* ctrl, int grid, int block, size_t smem, cudaStream_t st) {
+  void* args[] = {const_cast<DevParams*>(&P), &A_dev, &ctrl};
+  return cudaLaunchKernel(wave_kernel_fn(mode, batch), dim3(grid), dim3(block), args, smem, st);
+}
+
+}  // namespace OPTX_NS
+}  // namespace optx

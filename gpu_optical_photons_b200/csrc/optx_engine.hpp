@@ -1,0 +1,91 @@
+// optx_engine.hpp - internal interface between the C ABI (capi.cu) and the
+// kernels (kernels.cu, compiled once per math mode into namespaces optx::fast
+// and optx::exact). Not part of the public ABI (include/optx.h is).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "optx_device.cuh"
+
+namespace optx {
+
+// Tally binning as the kernels see it (transport.hpp:164-181 of the reference):
+// tscale = float(time_bins) / time_max, computed on the host in float.
+struct TallyDev {
+  uint32_t time_bins;
+  float tscale;
+  uint32_t xy_bins;
+  uint32_t len;  // 5 + time_bins + 1 + xy_bins^2 + 2
+};
+
+// Wavefront run description, resident in device memory (the host writes it
+// before each run; kernels read it, so a captured graph stays valid).
+struct WaveArgs {
+  const DevParams* params;              // event table (1 entry when not batched)
+  const unsigned long long* offsets;    // n_events + 1 relative photon offsets (batched)
+  uint32_t n_events;
+  uint32_t threshold;                   // refill a warp when fewer lanes than this are alive (1..32)
+  uint32_t cadence;                     // steps per photon per wave before a forced spill (0 = none)
+  uint32_t qcap;                        // capacity of each state queue, photons
+  unsigned long long total;             // photons in the run
+  unsigned long long first_id;          // Philox id of relative photon 0
+  unsigned long long wave_quota;        // fresh photons admitted per wave
+  float4* qa;                           // state queues: tiles of 32 photons x 4 float4 (64 B each)
+  float4* qb;
+  unsigned long long* tally;            // tally mode: n_events x len u64
+  TallyDev tc;
+  DevRecords rec;                       // records mode
+  const double* w_bin;                  // adjoint mode: time_bins + 1 weights
+  double w_det;
+  double inv_la, inv_la2, inv_ls, inv_ls2, inv_r, inv_tau, inv_tau2;
+  uint32_t score_mask;                  // bit j: parameter j has a score term
+  uint32_t pad;
+  double* grad;                         // adjoint mode: 4 FP64 sums (accumulated)
+  unsigned long long graph_handle;      // cudaGraphConditionalHandle of the wave loop, 0 = host loop
+  unsigned long long iter_cap;          // watchdog: max loop iterations per warp per wave
+};
+
+// Dynamic state of a wavefront run (device memory).
+struct WaveCtrl {
+  unsigned long long fresh_next;   // first fresh photon (relative index) of the current wave
+  unsigned long long useful;       // lane-steps that advanced a photon
+  unsigned long long issued;       // 32 x warp step iterations
+  unsigned int wave;               // current wave number
+  unsigned int n_in;               // survivors carried into the current wave
+  unsigned int fresh_count;        // fresh photons admitted in the current wave
+  unsigned int cursor;             // work items handed out (atomic)
+  unsigned int n_out;              // survivors spilled (atomic)
+  unsigned int blocks_done;        // blocks finished (atomic)
+  unsigned int active;             // 0 once the run is complete
+  unsigned int error;              // bit 0 queue overflow, bit 1 watchdog
+  unsigned int spills;             // total photons spilled over the run
+  unsigned int pad;
+};
+
+enum WaveMode : int { kModeTally = 0, kModeRecords = 1, kModeAdjoint = 2 };
+constexpr unsigned kErrQueue = 1u, kErrWatchdog = 2u;
+
+#define OPTX_DECLARE_LAUNCHERS(NS)                                                               \
+  namespace NS {                                                                                 \
+  cudaError_t launch_history_records(const DevParams& P, uint64_t first_id, uint64_t n,          \
+                                     const DevRecords& out, int block, cudaStream_t st);         \
+  cudaError_t launch_history_tally(const DevParams& P, const TallyDev& tc, uint64_t first_id,    \
+                                   uint64_t n, unsigned long long* tally, int block, int grid,   \
+                                   cudaStream_t st);                                             \
+  int history_tally_blocks_per_sm(int block, size_t smem);                                       \
+  /* Wavefront: prep (reset ctrl, zero tallies) and one wave. */                                 \
+  cudaError_t launch_wave_prep(const WaveArgs* A_dev, WaveCtrl* ctrl, int grid, int block,       \
+                               cudaStream_t st);                                                 \
+  const void* wave_prep_fn();                                                                    \
+  const void* wave_kernel_fn(int mode, bool batch);                                              \
+  int wave_blocks_per_sm(int mode, bool batch, int block, size_t smem);                          \
+  cudaError_t wave_set_smem(int mode, bool batch, size_t smem);                                  \
+  cudaError_t launch_wave(int mode, bool batch, const DevParams& P, const WaveArgs* A_dev,        \
+                          WaveCtrl* ctrl, int grid, int block, size_t smem, cudaStream_t st);    \
+  }
+
+OPTX_DECLARE_LAUNCHERS(fast)
+OPTX_DECLARE_LAUNCHERS(exact)
+
+}  // namespace optx

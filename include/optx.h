@@ -1,0 +1,186 @@
+/* optx.h - C ABI of the B200 optical-photon transport engine (liboptx.so).
+ *
+ * Drop-in boundary for the GPU path of the reference project
+ * zmeskma/GPU_Optical_photons (file:line below are relative to that project).
+ * Every entry point returns an int status (OPTX_OK = 0) and never throws;
+ * optx_last_error() gives the message of the calling thread's last failure.
+ * Plain pointers and sizes only: no C++ or torch types cross this boundary.
+ *
+ * Threading: calls from several host threads are serialised per device by the
+ * library. Host-buffer calls are synchronous (like the reference); the
+ * *_device calls are asynchronous on the given stream (NULL = legacy stream).
+ */
+#ifndef OPTX_H
+#define OPTX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OPTX_ABI_VERSION 1
+
+/* Status codes. */
+#define OPTX_OK 0
+#define OPTX_ERR_INVALID_ARGUMENT 1 /* reference: std::invalid_argument (gpu_event.cu:177-182) */
+#define OPTX_ERR_RUNTIME 2          /* reference: std::runtime_error (gpu_backend.cu:171-185) */
+#define OPTX_ERR_CUDA 3             /* reference: CUDA_CHECK -> runtime_error (cuda_util.cuh:17-24) */
+#define OPTX_ERR_NO_DEVICE 4
+#define OPTX_ERR_CAPACITY 5         /* a wavefront state queue overflowed */
+#define OPTX_ERR_WATCHDOG 6         /* a device loop hit its iteration cap */
+
+/* Math modes. FAST: CUDA logf/sincosf/cbrtf with FMA contraction (the
+ * reference's default GPU build). EXACT: portable log/sincos/cbrt and no FMA
+ * (the reference with OPTPHOT_PORTABLE_MATH and OPTPHOT_CUDA_FMAD=OFF); bit-
+ * identical to the reference CPU build with OPTPHOT_PORTABLE_MATH. */
+#define OPTX_MATH_FAST 0
+#define OPTX_MATH_EXACT 1
+
+/* optphot::SimParams, byte for byte (include/optphot/params.hpp:86-109). */
+typedef struct optx_params {
+  float hx, hy, hz;
+  float n_scint, n_det, n_out, abs_length, scat_length;
+  uint32_t surface; /* 0 polished, 1 black, 2 specular, 3 lambertian */
+  float reflectivity;
+  uint32_t source; /* 0 point, 1 uniform in the volume */
+  float src_x, src_y, src_z, tau;
+  uint32_t max_steps;
+  uint64_t seed;
+} optx_params;
+
+/* Extension (no reference counterpart): surface model and reflectivity per
+ * face 0..4 (0:-x 1:+x 2:-y 3:+y 4:-z); entry 5 (+z readout) is ignored. NULL
+ * everywhere it is accepted means `surface` / `reflectivity` on all five faces
+ * (params.hpp:60-66, transport.hpp:120-144). */
+typedef struct optx_faces {
+  uint32_t surface[6];
+  float reflectivity[6];
+} optx_faces;
+
+/* optphot::TallyConfig (include/optphot/transport.hpp:164-168). */
+typedef struct optx_tally_config {
+  uint32_t time_bins;
+  float time_max;
+  uint32_t xy_bins;
+} optx_tally_config;
+
+/* Caller-owned structure-of-arrays records, n entries each
+ * (optphot::PhotonRecords, include/optphot/backend.hpp:31-50). */
+typedef struct optx_records {
+  uint8_t* fate;
+  uint32_t* n_boundary;
+  uint32_t* n_scatter;
+  float *t, *x, *y, *z, *path;
+} optx_records;
+
+/* optphot::RunTiming (backend.hpp:65-71), milliseconds. */
+typedef struct optx_timing {
+  double total_ms, kernel_ms, h2d_ms, d2h_ms, alloc_ms;
+} optx_timing;
+
+/* optphot::EventStats (backend.hpp:95-103) plus wavefront counters. */
+typedef struct optx_event_stats {
+  uint64_t launches;          /* waves run (wave-kernel launches) */
+  uint64_t useful_lane_steps; /* photon steps done = sum of all photons' steps */
+  uint64_t issued_lane_steps; /* 32 x warp step iterations */
+  double kernels_ms;          /* device time of the transport */
+  uint64_t spills;            /* photons written to the state queue */
+} optx_event_stats;
+
+/* Wavefront engine configuration. Zero fields take defaults. */
+typedef struct optx_wave_config {
+  int32_t block_size;    /* threads per block, multiple of 32 (default 256) */
+  int32_t blocks_per_sm; /* persistent grid = blocks_per_sm x SMs (0: occupancy limit) */
+  uint32_t threshold;    /* refill a warp when fewer than this many lanes are alive, 1..32 (default 24) */
+  uint32_t cadence;      /* steps per photon per wave before a forced spill, 0 = none (default 0) */
+  uint64_t wave_quota;   /* fresh photons admitted per wave, 0 = all (default) */
+  int32_t use_graph;     /* 1: waves run as a CUDA-graph while loop (default); -1: host loop */
+  int32_t math;          /* OPTX_MATH_FAST / OPTX_MATH_EXACT */
+} optx_wave_config;
+
+/* ---- device ---------------------------------------------------------- */
+int optx_abi_version(void);
+/* reference: bool gpu_available() (backend.hpp:84) */
+int optx_gpu_available(void);
+/* reference: std::string gpu_device_name() (backend.hpp:85) */
+int optx_gpu_device_name(char* buf, size_t len);
+const char* optx_last_error(void);
+/* Frees the library's cached device / pinned buffers and graphs. */
+int optx_release_cache(void);
+
+/* ---- history kernel, host buffers (the reference's GPU calls) ---------- */
+/* reference: RunTiming run_gpu_records(const SimParams&, uint64_t n, PhotonRecords&,
+ *   int block_size = 256, uint64_t first_id = 0, uint64_t chunk = 1 << 24)
+ *   (backend.hpp:88-89; gpu_backend.cu:119-156). `out` holds n entries per array. */
+int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
+                     const optx_records* out, int block_size, uint64_t first_id, uint64_t chunk,
+                     int math, optx_timing* timing);
+/* reference: RunTiming run_gpu_tally(const SimParams&, const TallyConfig&, uint64_t n,
+ *   Tally&, int block_size = 256, uint64_t first_id = 0) (backend.hpp:90-91;
+ *   gpu_backend.cu:158-212). tally_out: flat u64 array of
+ *   5 + time_bins + 1 + xy_bins^2 + 2 entries = [fate counts | arrival-time histogram
+ *   (last bin overflow) | hit map, row-major iy*xy_bins+ix | sum n_boundary | sum n_scatter];
+ *   it is overwritten. */
+int optx_run_tally(const optx_params* p, const optx_faces* faces, const optx_tally_config* c,
+                   uint64_t n, uint64_t* tally_out, int block_size, uint64_t first_id, int math,
+                   optx_timing* timing);
+/* reference: RunTiming run_gpu_records_event(const SimParams&, uint64_t n, PhotonRecords&,
+ *   uint32_t steps_per_launch, int block_size = 256, uint64_t first_id = 0,
+ *   uint64_t chunk = 1 << 24, EventStats* = nullptr) (backend.hpp:110-115;
+ *   gpu_event.cu:174-244). Runs the wavefront engine with cadence = steps_per_launch:
+ *   each photon advances at most that many steps per wave. Records are bit-identical
+ *   to optx_run_records for every steps_per_launch, block_size and chunk. */
+int optx_run_records_event(const optx_params* p, const optx_faces* faces, uint64_t n,
+                           const optx_records* out, uint32_t steps_per_launch, int block_size,
+                           uint64_t first_id, uint64_t chunk, int math, optx_event_stats* stats,
+                           optx_timing* timing);
+
+/* ---- device-resident calls (caller device buffers, async on `stream`) --- */
+/* History records kernel into device arrays of n entries. */
+int optx_records_device(const optx_params* p, const optx_faces* faces, uint64_t n,
+                        uint64_t first_id, const optx_records* dev_out, int block_size, int math,
+                        void* stream);
+/* History tally kernel; ADDS into dev_tally (flat layout as optx_run_tally). */
+int optx_tally_device(const optx_params* p, const optx_faces* faces, const optx_tally_config* c,
+                      uint64_t n, uint64_t first_id, uint64_t* dev_tally, int block_size, int math,
+                      void* stream);
+
+/* ---- wavefront engine (extension: persistent, graph-captured, batched) -- */
+typedef struct optx_engine optx_engine;
+/* An engine for up to max_events events and max_photons photons per run. The
+ * tally layout is per event as in optx_run_tally. */
+int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t max_photons,
+                       const optx_wave_config* cfg, optx_engine** out);
+int optx_engine_destroy(optx_engine* e);
+/* Uploads a batch: events[i] (and faces[i] if faces != NULL) with counts[i] photons;
+ * event i owns photon ids first_id + sum(counts[0..i-1]) + k, k < counts[i], so its
+ * photons are those of the reference's run_cpu_* with first_id = that offset.
+ * Asynchronous on `stream` (host arrays are copied before return). */
+int optx_engine_set_events(optx_engine* e, const optx_params* events, const optx_faces* faces,
+                           const uint64_t* counts, uint32_t n_events, uint64_t first_id,
+                           void* stream);
+/* Runs the uploaded batch; per-event tallies stay on the device (overwritten).
+ * Asynchronous on `stream`. */
+int optx_engine_run_tally(optx_engine* e, void* stream);
+/* Runs the uploaded batch writing records (device arrays indexed by photon
+ * index relative to first_id, total entries = sum of counts). */
+int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* stream);
+/* Device pointer of the per-event tallies (n_events x tally length u64). */
+int optx_engine_tally_ptr(optx_engine* e, uint64_t** dev_ptr, uint64_t* len_per_event);
+/* Copies the per-event tallies to host memory (synchronises `stream`). */
+int optx_engine_get_tallies(optx_engine* e, uint64_t* host_out, void* stream);
+/* Statistics of the last run (synchronises `stream`). */
+int optx_engine_stats(optx_engine* e, optx_event_stats* stats, void* stream);
+/* One-shot batched run with host buffers: H2D of the event table, one graph
+ * launch, D2H of the per-event tallies (host_tallies: n_events x tally length). */
+int optx_run_batch(optx_engine* e, const optx_params* events, const optx_faces* faces,
+                   const uint64_t* counts, uint32_t n_events, uint64_t first_id,
+                   uint64_t* host_tallies, optx_event_stats* stats, optx_timing* timing);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPTX_H */

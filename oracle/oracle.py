@@ -1,0 +1,230 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+Loads ``oracle/liboptx_oracle.so`` (the project's restatement of the reference
+transport, oracle/optx_oracle.cpp) and, when present, ``oracle/_ref/libref_cpu*.so``
+(the reference's own CPU backend compiled from its sources by oracle/Makefile).
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
+this module; the engine in gpu_optical_photons_b200 never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboptx_oracle.so")
+REF_SO = {0: os.path.join(HERE, "_ref", "libref_cpu.so"),
+          1: os.path.join(HERE, "_ref", "libref_cpu_portable.so")}
+
+PLATFORM, PORTABLE, DOUBLE = 0, 1, 2
+
+_lib = None
+_ref = {}
+
+_P = ctypes.c_void_p
+_u64 = ctypes.c_uint64
+
+
+def build(with_ref: bool = True) -> None:
+    """Builds the oracle (and the reference backend when its checkout is present)."""
+    targets = ["all"]
+    if with_ref and os.path.isdir(os.environ.get("OPTX_REFERENCE", "/root/reference")):
+        targets.append("ref")
+    env = dict(os.environ)
+    env.setdefault("REF", os.environ.get("OPTX_REFERENCE", "/root/reference"))
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True, env=env)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build(with_ref=False)
+        L = ctypes.CDLL(ORACLE_SO)
+        L.oracle_records.restype = ctypes.c_int
+        L.oracle_records.argtypes = [_P, _P, _u64, _u64, ctypes.c_int, ctypes.c_int] + [_P] * 9
+        L.oracle_tally.argtypes = [_P, _P, _P, _u64, _u64, ctypes.c_int, ctypes.c_int, _P]
+        L.oracle_batch_tally.argtypes = [_P, _P, ctypes.c_uint32, _P, ctypes.c_int, ctypes.c_int, _P]
+        L.oracle_adjoint.argtypes = [_P, _P, _u64, _u64, ctypes.c_int, ctypes.c_int, _P,
+                                     ctypes.c_double, _P, _P, _P]
+        L.oracle_opcount.argtypes = [_P, _P, _u64, _u64, _P]
+        L.oracle_stream.argtypes = [_u64, _u64, ctypes.c_uint32, ctypes.c_uint32, _P]
+        L.oracle_philox.argtypes = [_P, _P, _P]
+        L.oracle_u32_to_uniform.restype = ctypes.c_float
+        L.oracle_u32_to_uniform.argtypes = [ctypes.c_uint32]
+        L.oracle_portable_log.restype = ctypes.c_float
+        L.oracle_portable_log.argtypes = [ctypes.c_float]
+        L.oracle_portable_cbrt.restype = ctypes.c_float
+        L.oracle_portable_cbrt.argtypes = [ctypes.c_float]
+        L.oracle_portable_sincos_turns.argtypes = [ctypes.c_float, _P, _P]
+        L.oracle_fresnel.restype = ctypes.c_float
+        L.oracle_fresnel.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_float]
+        L.oracle_rayleigh_cos.restype = ctypes.c_float
+        L.oracle_rayleigh_cos.argtypes = [ctypes.c_float, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def ref_available(mode: int = PLATFORM) -> bool:
+    return os.path.exists(REF_SO[mode])
+
+
+def ref(mode: int = PLATFORM):
+    if mode not in _ref:
+        L = ctypes.CDLL(REF_SO[mode])
+        L.ref_records.restype = ctypes.c_double
+        L.ref_records.argtypes = [_P, _u64, _u64, ctypes.c_int] + [_P] * 8
+        L.ref_tally.restype = ctypes.c_double
+        L.ref_tally.argtypes = [_P, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32, _u64, _u64,
+                                ctypes.c_int, _P]
+        L.ref_philox.argtypes = [_P, _P, _P]
+        L.ref_max_threads.restype = ctypes.c_int
+        L.ref_portable_math.restype = ctypes.c_int
+        _ref[mode] = L
+    return _ref[mode]
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class Records(dict):
+    """Structure-of-arrays photon records (backend.hpp:31-50 field set)."""
+
+    FIELDS = ("fate", "n_boundary", "n_scatter", "t", "x", "y", "z", "path")
+
+    @staticmethod
+    def empty(n: int) -> "Records":
+        r = Records()
+        r["fate"] = np.zeros(n, np.uint8)
+        r["n_boundary"] = np.zeros(n, np.uint32)
+        r["n_scatter"] = np.zeros(n, np.uint32)
+        for k in ("t", "x", "y", "z", "path"):
+            r[k] = np.zeros(n, np.float32)
+        return r
+
+    def steps(self) -> np.ndarray:
+        """Photon steps = n_boundary + n_scatter + [absorbed in bulk] (optphot_event_bench.cpp:39-41)."""
+        return (self["n_boundary"].astype(np.int64) + self["n_scatter"]
+                + (self["fate"] == 1))
+
+
+def records(p, n: int, first_id: int = 0, mode: int = PLATFORM, threads: int = 0,
+            draws: bool = False) -> Records:
+    """Oracle records for photons first_id .. first_id + n - 1."""
+    r = Records.empty(n)
+    d = np.zeros(n, np.uint32) if draws else None
+    cp = p.to_c()
+    faces = p.faces_c()
+    lib().oracle_records(ctypes.byref(cp), ctypes.byref(faces) if faces is not None else None,
+                         n, first_id, mode, threads,
+                         *[_ptr(r[k]) for k in Records.FIELDS], _ptr(d))
+    if draws:
+        r["draws"] = d
+    return r
+
+
+def tally(p, c, n: int, first_id: int = 0, mode: int = PLATFORM, threads: int = 0) -> np.ndarray:
+    out = np.zeros(c.length, np.uint64)
+    cp, cc = p.to_c(), c.to_c()
+    faces = p.faces_c()
+    lib().oracle_tally(ctypes.byref(cp), ctypes.byref(faces) if faces is not None else None,
+                       ctypes.byref(cc), n, first_id, mode, threads, _ptr(out))
+    return out
+
+
+def batch_tally(events_c, offsets: np.ndarray, c, mode: int = PLATFORM, threads: int = 0,
+                n_events: int | None = None) -> np.ndarray:
+    """Per-event tallies; events_c is a ctypes array of CSimParams, offsets uint64[n+1]."""
+    ne = len(offsets) - 1 if n_events is None else n_events
+    out = np.zeros((ne, c.length), np.uint64)
+    cc = c.to_c()
+    offs = np.ascontiguousarray(offsets, dtype=np.uint64)
+    lib().oracle_batch_tally(ctypes.cast(events_c, ctypes.c_void_p), _ptr(offs), ne,
+                             ctypes.byref(cc), mode, threads, _ptr(out))
+    return out
+
+
+def adjoint(p, c, n: int, w_bin=None, w_det: float = 0.0, first_id: int = 0,
+            mode: int = PLATFORM, threads: int = 0):
+    """FP64 score-function gradient sum_photons w * S (see oracle_adjoint)."""
+    grad = np.zeros(4, np.float64)
+    hist = np.zeros(c.time_bins + 1, np.uint64)
+    det = np.zeros(1, np.uint64)
+    wb = None if w_bin is None else np.ascontiguousarray(w_bin, np.float64)
+    cp, cc = p.to_c(), c.to_c()
+    lib().oracle_adjoint(ctypes.byref(cp), ctypes.byref(cc), n, first_id, mode, threads,
+                         _ptr(wb), float(w_det), _ptr(grad), _ptr(hist), _ptr(det))
+    return grad, hist, int(det[0])
+
+
+STEP_KINDS = ["start", "absorb", "scatter", "readout_reflect", "detect", "polished_reflect",
+              "escape", "black", "painted_absorb", "specular", "lambertian"]
+
+
+def opcount(p, n: int, first_id: int = 0) -> dict:
+    """Algorithmic op counts per step kind: {kind: (steps, fp, transcendental, int)}."""
+    out = np.zeros(len(STEP_KINDS) * 4, np.uint64)
+    cp = p.to_c()
+    faces = p.faces_c()
+    lib().oracle_opcount(ctypes.byref(cp), ctypes.byref(faces) if faces is not None else None,
+                         n, first_id, _ptr(out))
+    out = out.reshape(-1, 4)
+    return {k: tuple(int(v) for v in out[i]) for i, k in enumerate(STEP_KINDS)}
+
+
+def stream(seed: int, photon_id: int, n: int, skip: int = 0) -> np.ndarray:
+    out = np.zeros(n, np.uint32)
+    lib().oracle_stream(seed, photon_id, skip, n, _ptr(out))
+    return out
+
+
+def philox(ctr, key) -> np.ndarray:
+    c = np.ascontiguousarray(ctr, np.uint32)
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.zeros(4, np.uint32)
+    lib().oracle_philox(_ptr(c), _ptr(k), _ptr(out))
+    return out
+
+
+# ---- the reference's own CPU backend (oracle/_ref) -------------------------
+
+def ref_records(p, n: int, first_id: int = 0, mode: int = PLATFORM, threads: int = 0):
+    r = Records.empty(n)
+    cp = p.to_c()
+    ms = ref(mode).ref_records(ctypes.byref(cp), n, first_id, threads,
+                               *[_ptr(r[k]) for k in Records.FIELDS])
+    return r, ms
+
+
+def ref_tally(p, c, n: int, first_id: int = 0, mode: int = PLATFORM, threads: int = 0):
+    out = np.zeros(c.length, np.uint64)
+    cp = p.to_c()
+    ms = ref(mode).ref_tally(ctypes.byref(cp), c.time_bins, c.time_max, c.xy_bins, n, first_id,
+                             threads, _ptr(out))
+    return out, ms
+
+
+def ref_philox(ctr, key, mode: int = PLATFORM) -> np.ndarray:
+    c = np.ascontiguousarray(ctr, np.uint32)
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.zeros(4, np.uint32)
+    ref(mode).ref_philox(_ptr(c), _ptr(k), _ptr(out))
+    return out
+
+
+def compare_histories(a: Records, b: Records) -> dict:
+    """Photon-by-photon agreement (reference src/core/compare.cpp:103-127)."""
+    discrete = ((a["fate"] == b["fate"]) & (a["n_boundary"] == b["n_boundary"])
+                & (a["n_scatter"] == b["n_scatter"]))
+    same_bits = discrete.copy()
+    for k in ("t", "x", "y", "z", "path"):
+        same_bits &= a[k].view(np.uint32) == b[k].view(np.uint32)
+    n = len(a["fate"])
+    bad = np.nonzero(~discrete)[0]
+    return {"n": n, "bitwise_identical": int(same_bits.sum()), "same_discrete": int(discrete.sum()),
+            "fate_differs": int((a["fate"] != b["fate"]).sum()),
+            "first_divergent": int(bad[0]) if len(bad) else -1}

@@ -1,0 +1,110 @@
+"""Wavefront engine through the C ABI: bit identity with the history kernel (the
+property of the reference's tests/test_gpu.cpp:160-212), integer tallies, graph vs
+host loop, batched events against the oracle."""
+import numpy as np
+import pytest
+
+from gpu_optical_photons_b200 import params as P
+from gpu_optical_photons_b200.wavefront import WaveConfig, WavefrontEngine, batched_events
+from helpers import compare_histories, chi2_two_sample, steps_of
+
+pytestmark = pytest.mark.gpu
+
+SETUPS = {
+    "polished": P.SimParams(scat_length=300.0),
+    "lambertian": P.SimParams(surface=P.LAMBERTIAN, reflectivity=0.95, n_det=1.5, source=P.VOLUME),
+    "capped": P.SimParams(scat_length=300.0, max_steps=5),
+}
+
+
+@pytest.mark.parametrize("setup", list(SETUPS))
+@pytest.mark.parametrize("k", [1, 3, 100000])
+def test_event_records_identical_to_history(engine, setup, k):
+    p = SETUPS[setup]
+    n = 100_003
+    hist, _ = engine.run_gpu_records(p, n)
+    ev, st, _ = engine.run_gpu_records_event(p, n, k, 64, 0, 30011)
+    assert compare_histories(hist, ev)["bitwise_identical"] == n
+    assert st["useful_lane_steps"] == int(steps_of(hist).sum())
+    assert st["issued_lane_steps"] >= st["useful_lane_steps"]
+
+
+@pytest.mark.parametrize("cfg", [
+    WaveConfig(threshold=1), WaveConfig(threshold=32), WaveConfig(threshold=16, cadence=4),
+    WaveConfig(threshold=24, wave_quota=50_000), WaveConfig(block_size=128, threshold=8),
+    WaveConfig(use_graph=False, threshold=20, cadence=7, wave_quota=30_000)])
+@pytest.mark.parametrize("math_mode", ["exact", "fast"])
+def test_wavefront_tally_equals_history_tally(engine, cfg, math_mode):
+    p = P.config2()[0]
+    c = P.TallyConfig(500, 50.0, 50)
+    n = 400_000
+    cfg = WaveConfig(**{**cfg.__dict__, "math": math_mode})
+    _, fh, _ = engine.run_gpu_tally(p, c, n, math=math_mode)
+    eng = WavefrontEngine(c, 1, n, cfg)
+    eng.set_events([p], [n])
+    eng.run_tally()
+    fw = eng.tallies()[0]
+    st = eng.stats()
+    eng.close()
+    assert np.array_equal(fh, fw)
+    assert st["useful_lane_steps"] == int(fh[-2] + fh[-1] + fh[1])
+
+
+def test_wavefront_records_through_engine(engine):
+    import torch
+    p = P.config3(True)[0]
+    n = 200_000
+    hist, _ = engine.run_gpu_records(p, n, first_id=5)
+    eng = WavefrontEngine(P.TallyConfig(), 1, n, WaveConfig(threshold=24, cadence=16))
+    eng.set_events([p], [n], first_id=5)
+    d = engine.device_records(n)
+    eng.run_records(d, stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    rec = engine.records_to_numpy(d)
+    eng.close()
+    assert compare_histories(hist, rec)["bitwise_identical"] == n
+
+
+def test_batched_events_exact_equals_oracle(engine, oracle):
+    events, counts = batched_events(n_events=48, seed=7, median=2000, n_min=1, n_max=20000)
+    counts[3] = 0  # an empty event
+    counts[10] = 1
+    c = P.TallyConfig(100, 50.0, 10)
+    eng = WavefrontEngine(c, len(events), int(counts.sum()), WaveConfig(math="exact", threshold=24))
+    eng.set_events(events, counts, first_id=1000)
+    eng.run_tally()
+    got = eng.tallies()
+    eng.close()
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64) + np.uint64(1000)
+    arr = (P.CSimParams * len(events))(*[e.to_c() for e in events])
+    ref = oracle.batch_tally(arr, offs, c, mode=oracle.PORTABLE)
+    assert np.array_equal(got, ref)
+
+
+def test_batched_events_fast_vs_oracle(engine, oracle):
+    events, counts = batched_events(n_events=64, seed=11, median=5000)
+    c = P.TallyConfig(100, 50.0, 10)
+    eng = WavefrontEngine(c, len(events), int(counts.sum()))
+    got, st, tm = eng.run_batch(events, counts)
+    eng.close()
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
+    arr = (P.CSimParams * len(events))(*[e.to_c() for e in events])
+    ref = oracle.batch_tally(arr, offs, c, mode=oracle.PLATFORM)
+    assert np.array_equal(got[:, :5].sum(1), counts)
+    # per-event detected counts agree to the floating-point divergence tolerance
+    assert np.abs(got[:, 0].astype(np.int64) - ref[:, 0].astype(np.int64)).sum() <= 0.001 * counts.sum()
+    chi2, ndf, pv = chi2_two_sample(got[:, 5:106].sum(0), ref[:, 5:106].sum(0))
+    assert pv > 0.01
+
+
+def test_graph_and_host_loop_agree(engine):
+    events, counts = batched_events(n_events=32, seed=3, median=3000)
+    c = P.TallyConfig(100, 50.0, 10)
+    out = []
+    for g in (True, False):
+        eng = WavefrontEngine(c, 32, int(counts.sum()), WaveConfig(use_graph=g, wave_quota=20000))
+        eng.set_events(events, counts)
+        eng.run_tally()
+        out.append(eng.tallies())
+        eng.close()
+    assert np.array_equal(out[0], out[1])
