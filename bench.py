@@ -1,0 +1,347 @@
+"""Benchmark of the batched optical-photon transport on B200.
+
+Workload: 4096 events with lognormal photon counts (median 1e4, sigma 1, clamped
+to [1e2, 1e6]; 66,481,565 photons, ~2.8e8 photon-steps), per-event absorption
+length, reflectivity, refractive index and scattering length, point sources
+uniform in a 50 mm cube, Lambertian faces, per-event tallies (100 arrival-time
+bins over 0-50 ns + overflow, 10x10 hit map). A step is one run of the whole
+batch: one CUDA-graph launch of the persistent wavefront engine.
+
+  value  photon-steps/s with the event table resident on the device
+  e2e    photon-steps/s through the C ABI call optx_run_batch with pinned host
+         buffers: H2D of the event table and D2H of the per-event tallies inside
+         the timed region
+
+``--impl reference`` times the reference's own CPU implementation
+(run_cpu_tally of the reference backend, compiled from its sources into
+oracle/_ref; the oracle port when that is absent) on the same workload.
+Multi-GPU (torchrun): every rank runs its own copy of the batch (independent
+events, no collective on the data path), value = all ranks' steps / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "photon-steps/s (batched wavefront, 4096 events)"
+UNIT = "photon-steps/s"
+# Algorithmic work per photon-step of this workload: 250.2 scalar ops (91.0 FP32
+# arithmetic/compare, 3.63 log/sin/cos/cbrt calls, 155.6 Philox/uniform integer
+# ops), counted by the oracle's op-counting scalar type over 64 events x 500
+# photons (tests/test_opcount.py checks this constant against the oracle).
+OPS_PER_STEP = 250.2
+# State-queue bytes per spilled photon: one 64-byte write and one 64-byte read.
+QUEUE_BYTES_PER_SPILL = 128
+SMS, FP32_LANES_PER_SM = 148, 128
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="optx", choices=["optx", "reference"])
+    ap.add_argument("--threshold", type=int, default=0, help="0: tuned default")
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--events", type=int, default=4096)
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        backend = "nccl" if args.impl == "optx" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def steps_of_tallies(t: np.ndarray) -> int:
+    """photon-steps = sum n_boundary + sum n_scatter + absorbed in bulk (per event rows)."""
+    t = np.asarray(t, dtype=np.uint64).reshape(-1, t.shape[-1])
+    return int(t[:, -2].sum() + t[:, -1].sum() + t[:, 1].sum())
+
+
+def cpu_reference_leg(events, counts, tc, max_events: int, threads: int = 0, first: int = 0):
+    """Reference CPU tally (oracle/_ref) or the oracle port over events first .. max_events-1."""
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
+    steps = 0
+    photons = 0
+    t0 = time.perf_counter()
+    for i in range(first, max_events):
+        if kind == "reference":
+            t, _ = O.ref_tally(events[i], tc, int(counts[i]), int(offs[i]), threads=threads)
+        else:
+            t = O.tally(events[i], tc, int(counts[i]), int(offs[i]), threads=threads)
+        steps += steps_of_tallies(t[None, :])
+        photons += int(counts[i])
+    dt = time.perf_counter() - t0
+    cores = (O.ref(0).ref_max_threads() if kind == "reference" else os.cpu_count()) if threads == 0 else threads
+    return {"value": steps / dt, "unit": UNIT, "cores": int(cores), "kind": kind,
+            "sample": f"events {first}..{max_events - 1} of {len(counts)} ({photons} photons, {steps} photon-steps), "
+                      f"run_cpu_tally per event, {dt:.1f} s"}, steps / dt
+
+
+def run_reference(args):
+    # The reference is a CPU code: rank 0 alone runs it; other ranks exit at once.
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from gpu_optical_photons_b200.params import TallyConfig
+    from gpu_optical_photons_b200.wavefront import batched_events
+    events, counts = batched_events(n_events=args.events)
+    tc = TallyConfig(100, 50.0, 10)
+    per_step = min(512, len(events))
+    vals = []
+    for s in range(args.warmup + args.steps):
+        lo = (s * per_step) % len(events)
+        base, v = cpu_reference_leg(events, counts, tc, lo + per_step, first=lo)
+        if s >= args.warmup:
+            vals.append(v)
+    value = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched events ({args.events}), reference CPU run_cpu_tally",
+                       "per_step_sample": f"{per_step} events"},
+            "cpu_baseline": {**base, "value": value,
+                             "sample": f"{per_step} consecutive events per step; " + base["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_optx(args):
+    import torch
+    world, rank, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    from gpu_optical_photons_b200 import build
+    build.build()
+    import gpu_optical_photons_b200 as g
+    from gpu_optical_photons_b200 import _lib
+    from gpu_optical_photons_b200.params import CSimParams, TallyConfig
+    from gpu_optical_photons_b200.wavefront import WaveConfig, WavefrontEngine, batched_events
+
+    events, counts = batched_events(n_events=args.events)
+    n_photons = int(counts.sum())
+    tc = TallyConfig(100, 50.0, 10)
+    cfg = WaveConfig(block_size=args.block or 256, threshold=args.threshold or 24)
+    eng = WavefrontEngine(tc, len(events), n_photons, cfg)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    # Pinned host buffers for the e2e leg.
+    arr = (CSimParams * len(events))(*[e.to_c() for e in events])
+    ev_pinned = torch.empty(ctypes.sizeof(arr), dtype=torch.uint8, pin_memory=True)
+    ctypes.memmove(ev_pinned.data_ptr(), ctypes.addressof(arr), ctypes.sizeof(arr))
+    cnt_pinned = torch.from_numpy(counts.astype(np.int64)).pin_memory()
+    out_pinned = torch.empty((len(events), tc.length), dtype=torch.int64, pin_memory=True)
+    h2d_bytes = len(events) * 112 + (len(events) + 1) * 8 + 256   # DevParams table + offsets + run args
+    d2h_bytes = len(events) * tc.length * 8 + 64                  # tallies + control block
+
+    eng.set_events(events, counts, 0, stream=sptr)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    # warm-up
+    for _ in range(args.warmup):
+        eng.run_tally(stream=sptr)
+    torch.cuda.synchronize()
+    st0 = eng.stats(stream=sptr)
+    tallies = eng.tallies(stream=sptr)
+    steps_per_run = steps_of_tallies(tallies)
+    assert int(tallies[:, :5].sum()) == n_photons
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_wall = time.perf_counter()
+        for k in range(args.steps):
+            flush.zero_()                       # L2 flush between timed steps (outside the events)
+            starts[k].record(stream)
+            eng.run_tally(stream=sptr)
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t_wall
+    if pg:
+        pg.barrier()
+    dev_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms_step = sum(dev_ms) / args.steps
+    st = eng.stats(stream=sptr)
+    waves = int(st["launches"])
+    if pg:
+        t = torch.tensor([ms_step], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * steps_per_run / (ms_step * 1e-3)
+
+    # e2e: the C ABI call with host buffers (H2D table, run, D2H tallies) per step.
+    L = _lib.lib()
+    sts = _lib.CEventStats()
+    tmg = _lib.CTiming()
+    e2e_ms = []
+    for k in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _lib.check(L.optx_run_batch(eng._h, ctypes.c_void_p(ev_pinned.data_ptr()), None,
+                                    ctypes.c_void_p(cnt_pinned.data_ptr()), len(events), 0,
+                                    ctypes.c_void_p(out_pinned.data_ptr()), ctypes.byref(sts),
+                                    ctypes.byref(tmg)))
+        dt = (time.perf_counter() - t0) * 1e3
+        if k >= args.warmup:
+            e2e_ms.append(dt)
+    e2e_step = float(np.mean(e2e_ms))
+    if pg:
+        t = torch.tensor([e2e_step], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_step = float(t.item())
+    assert np.array_equal(out_pinned.numpy().astype(np.uint64), tallies)
+
+    clocks = clk.summary()
+    peak_mhz = clocks["sm_max_mhz"] or 1965.0
+    peak_gops = SMS * FP32_LANES_PER_SM * peak_mhz * 1e6 / 1e9
+    achieved_gops = OPS_PER_STEP * steps_per_run / (ms_step * 1e-3) / 1e9
+    traffic = None
+    prof = os.path.join(HERE, "profiles", "wave_kernel_batched.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            bps = json.load(f).get("dram_bytes_per_photon_step")
+        if bps:
+            traffic = bps * steps_per_run
+    queue_bytes = QUEUE_BYTES_PER_SPILL * int(st["spills"])
+    peaks = {}
+    peaks_path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peaks = json.load(f)
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded event generator)",
+        "config": {"workload": "batched events: 4096 events, lognormal photons/event (median 1e4, "
+                               "sigma 1, [1e2,1e6]), Lambertian cube, per-event tallies",
+                   "events": len(events), "photons_per_step": n_photons,
+                   "photon_steps_per_step": steps_per_run, "photons_per_s": world * n_photons / (ms_step * 1e-3),
+                   "l2": "flushed between timed steps (256 MB write, outside the CUDA events)",
+                   "engine": {"block_size": cfg.block_size, "threshold": cfg.threshold,
+                              "cadence": cfg.cadence, "graph": True, "math": cfg.math},
+                   "parallelism": f"dp{world} (independent event batches per GPU)"},
+        "e2e": {"value": world * steps_per_run / (e2e_step * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
+                "ms_per_step": e2e_step, "call": "optx_run_batch (pinned host buffers)"},
+        "gpu_launches": args.steps * (waves + 1),
+        "waves_per_step": waves,
+        "simt_efficiency": st["simt_efficiency"],
+        "roofline": {"bound": "issue", "achieved": achieved_gops, "peak": peak_gops, "unit": "Gop/s",
+                     "frac": achieved_gops / peak_gops, "traffic": traffic,
+                     "peak_source": f"nominal FP32 lane issue rate {SMS} SMs x {FP32_LANES_PER_SM} lanes x "
+                                    f"{peak_mhz:.0f} MHz (max SM clock seen); no measured issue peak exists",
+                     "ops_per_photon_step": OPS_PER_STEP,
+                     "hbm": {"queue_bytes_per_step": queue_bytes,
+                             "achieved_gbs": queue_bytes / (ms_step * 1e-3) / 1e9,
+                             "peak_gbs": hbm_peak,
+                             "frac": queue_bytes / (ms_step * 1e-3) / 1e9 / hbm_peak,
+                             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"}},
+        "clocks": clocks,
+        "wall_s_timed": wall,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        base, _ = cpu_reference_leg(events, counts, tc, max_events=min(1024, len(events)))
+        line["cpu_baseline"] = base
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_optx(a)

@@ -349,6 +349,14 @@ int engine_upload_args(optx_engine* e, int mode, bool batch, int grid, cudaGraph
   for (const DevParams& p : e->h_params) max_steps = std::max(max_steps, p.max_steps);
   a.iter_cap = (static_cast<unsigned long long>(e->total) + e->qcap + 64ull) *
                    (static_cast<unsigned long long>(max_steps) + 2ull) + 4096ull;
+  // Every photon of a wave steps at least once, so a run needs at most about
+  // (admission waves) + max_steps waves; the cap only stops a broken run.
+  const unsigned long long per_wave = std::max<unsigned long long>(
+      1ull, std::min<unsigned long long>(a.wave_quota, e->cfg.cadence ? e->qcap / 2 : a.wave_quota));
+  const unsigned long long cap =
+      4ull * (max_steps + 2ull) + 4ull * (e->total / per_wave) + 64ull;
+  a.wave_cap = static_cast<uint32_t>(std::min<unsigned long long>(std::max(cap, 100000ull), 0xfffffff0ull));
+  a.use_graph = (e->cfg.use_graph >= 0) ? 1u : 0u;
   (void)grid;
   (void)batch;
   OPTX_CUDA(cudaMemcpyAsync(e->d_args, &a, sizeof(a), cudaMemcpyHostToDevice, st));
@@ -446,8 +454,7 @@ int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_
       OPTX_CUDA(cudaMemcpyAsync(&active, &e->d_ctrl->active, sizeof(active),
                                 cudaMemcpyDeviceToHost, st));
       OPTX_CUDA(cudaStreamSynchronize(st));
-      if (!active) break;
-      if (w > (1ull << 24)) return fail(OPTX_ERR_WATCHDOG, "wavefront did not finish");
+      if (!active) break;  // the kernel stops the run itself at its wave cap
     }
     OPTX_CUDA(cudaEventRecord(e->ev1, st));
   }

@@ -236,6 +236,7 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
   ScoreAux aux{0u, 0.0f};
   uint32_t pidx = 0u, ev = 0u;
   bool alive = false, exhausted = false;
+  bool refilled = false;  // warp-uniform: lanes were loaded and have not stepped yet
   uint32_t wsteps = 0u;
   // Per-lane tallies (flushed at the end; batched: when the lane's event changes).
   uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0;
@@ -337,6 +338,7 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
         base = __shfl_sync(kFull, base, 0);
         const uint32_t got = base >= items ? 0u : min(need, items - base);
         exhausted = got < need;
+        refilled = got > 0u;
         const uint32_t rank = static_cast<uint32_t>(__popc(~amask & lt));
         if (!alive && rank < got) {
           const uint32_t item = base + rank;
@@ -373,7 +375,9 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
       if (exhausted) {
         const uint32_t na = static_cast<uint32_t>(__popc(amask));
         if (na == 0u) break;
-        if (na < T) {
+        // Spill only photons that have stepped in this wave, so that every
+        // item of a wave makes progress and the run always ends.
+        if (na < T && !refilled) {
           spill_lanes(alive);
           alive = false;
           break;
@@ -395,6 +399,7 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
         finish(kMaxSteps, P);
       }
     }
+    refilled = false;
     issued += 32u;
     useful += static_cast<uint32_t>(__popc(amask));
     if (cadence != 0u) {  // forced compaction after `cadence` steps in this wave
@@ -477,10 +482,11 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
       vc->blocks_done = 0u;
       vc->spills = vc->spills + n_out;
       vc->wave = vc->wave + 1u;
+      if (vc->wave >= A->wave_cap && (n_out + fresh) > 0ull) vc->error = vc->error | kErrWatchdog;
       const bool more = (n_out + fresh) > 0ull && vc->error == 0u;
       vc->active = more ? 1u : 0u;
       __threadfence();
-      if (!more && A->graph_handle != 0ull) cudaGraphSetConditional(A->graph_handle, 0u);
+      if (!more && A->use_graph != 0u) cudaGraphSetConditional(A->graph_handle, 0u);
     }
   }
 }

