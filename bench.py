@@ -50,13 +50,17 @@ SMS, FP32_LANES_PER_SM = 148, 128
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="optx", choices=["optx", "reference"])
     ap.add_argument("--threshold", type=int, default=0, help="0: tuned default")
     ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--bps", type=int, default=0, help="resident blocks per SM (register budget)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--events", type=int, default=4096)
+    ap.add_argument("--host-loop", action="store_true",
+                    help="launch the waves from the host instead of the graph while loop "
+                         "(same kernels; used for per-kernel profiling)")
     return ap.parse_args()
 
 
@@ -78,7 +82,7 @@ def dist_setup(args):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -93,7 +97,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -203,7 +207,8 @@ def run_optx(args):
     events, counts = batched_events(n_events=args.events)
     n_photons = int(counts.sum())
     tc = TallyConfig(100, 50.0, 10)
-    cfg = WaveConfig(block_size=args.block or 256, threshold=args.threshold or 24)
+    cfg = WaveConfig(block_size=args.block or 256, threshold=args.threshold or 28,
+                     blocks_per_sm=args.bps, use_graph=not args.host_loop)
     eng = WavefrontEngine(tc, len(events), n_photons, cfg)
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
@@ -307,7 +312,8 @@ def run_optx(args):
                    "photon_steps_per_step": steps_per_run, "photons_per_s": world * n_photons / (ms_step * 1e-3),
                    "l2": "flushed between timed steps (256 MB write, outside the CUDA events)",
                    "engine": {"block_size": cfg.block_size, "threshold": cfg.threshold,
-                              "cadence": cfg.cadence, "graph": True, "math": cfg.math},
+                              "blocks_per_sm": cfg.blocks_per_sm,
+                              "cadence": cfg.cadence, "graph": cfg.use_graph, "math": cfg.math},
                    "parallelism": f"dp{world} (independent event batches per GPU)"},
         "e2e": {"value": world * steps_per_run / (e2e_step * 1e-3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,

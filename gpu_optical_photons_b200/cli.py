@@ -1,0 +1,107 @@
+"""Command-line runner (the role of the reference's apps/optphot_main.cpp and
+apps/optphot_event_bench.cpp): runs one configuration through the history or
+the wavefront kernel and prints a JSON line with timings and tallies summary.
+
+    python -m gpu_optical_photons_b200.cli --config config2 --engine wave --n 1e7
+    python -m gpu_optical_photons_b200.cli --config config1 --engine history --mode records --n 1e6
+
+Options mirror the reference's physics keys (--n_det, --abs_length, ...).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import params as P
+
+
+CONFIGS = {"default": lambda: (P.SimParams(), P.TallyConfig()),
+           "config1": P.config1, "config2": P.config2, "config3": P.config3,
+           "config3_ref": lambda: P.config3(False)}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--config", default="config1", choices=sorted(CONFIGS))
+    ap.add_argument("--engine", default="history", choices=["history", "wave"])
+    ap.add_argument("--mode", default="tally", choices=["tally", "records"])
+    ap.add_argument("--n", type=float, default=1e6)
+    ap.add_argument("--math", default="fast", choices=["fast", "exact"])
+    ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--threshold", type=int, default=24)
+    ap.add_argument("--cadence", type=int, default=0)
+    ap.add_argument("--host-loop", action="store_true", help="launch waves from the host (no graph)")
+    ap.add_argument("--repeat", type=int, default=3)
+    for key in ("n_scint", "n_det", "n_out", "abs_length", "scat_length", "reflectivity", "tau",
+                "src_x", "src_y", "src_z"):
+        ap.add_argument(f"--{key}", type=float)
+    ap.add_argument("--seed", type=int)
+    ap.add_argument("--max_steps", type=int)
+    a = ap.parse_args(argv)
+
+    import torch
+    import gpu_optical_photons_b200 as g
+    from .wavefront import WaveConfig, WavefrontEngine
+
+    p, c = CONFIGS[a.config]()
+    for key in ("n_scint", "n_det", "n_out", "abs_length", "scat_length", "reflectivity", "tau",
+                "src_x", "src_y", "src_z", "seed", "max_steps"):
+        v = getattr(a, key)
+        if v is not None:
+            setattr(p, key, v)
+    n = int(a.n)
+    out = {"config": a.config, "engine": a.engine, "mode": a.mode, "n": n, "math": a.math,
+           "device": g.gpu_device_name()}
+    times = []
+    if a.engine == "history":
+        if a.mode == "tally":
+            dev = torch.zeros(c.length, dtype=torch.int64, device="cuda")
+            for _ in range(a.repeat):
+                dev.zero_()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                g.tally_device(p, c, n, out=dev, block_size=a.block, math=a.math)
+                torch.cuda.synchronize()
+                times.append((time.perf_counter() - t0) * 1e3)
+            flat = dev.cpu().numpy().astype(np.uint64)
+        else:
+            rec = g.device_records(n)
+            for _ in range(a.repeat):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                g.records_device(p, n, out=rec, block_size=a.block, math=a.math)
+                torch.cuda.synchronize()
+                times.append((time.perf_counter() - t0) * 1e3)
+            r = g.records_to_numpy(rec)
+            flat = None
+            out["steps"] = int(r.steps().sum())
+    else:
+        cfg = WaveConfig(block_size=a.block, threshold=a.threshold, cadence=a.cadence,
+                         use_graph=not a.host_loop, math=a.math)
+        eng = WavefrontEngine(c, 1, n, cfg)
+        eng.set_events([p], [n])
+        for _ in range(a.repeat):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.run_tally()
+            torch.cuda.synchronize()
+            times.append((time.perf_counter() - t0) * 1e3)
+        flat = eng.tallies()[0]
+        out["stats"] = eng.stats()
+        eng.close()
+    if flat is not None:
+        t = g.Tally.from_flat(flat, c)
+        out["fates"] = [int(v) for v in t.fate_counts]
+        out["steps"] = t.steps()
+    best = min(times)
+    out["ms"] = best
+    out["photons_per_s"] = n / (best * 1e-3)
+    out["photon_steps_per_s"] = out["steps"] / (best * 1e-3)
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -263,6 +263,7 @@ struct optx_engine {
   WaveCtrl* d_ctrl = nullptr;
   DevParams* d_params = nullptr;
   unsigned long long* d_offsets = nullptr;
+  uint32_t* d_evtable = nullptr;
   float4* d_qa = nullptr;
   float4* d_qb = nullptr;
   unsigned long long* d_tally = nullptr;
@@ -293,18 +294,26 @@ struct optx_engine {
 namespace {
 
 size_t wave_smem(const optx_engine* e, int mode, bool batch) {
-  if (mode == kModeTally && !batch) return static_cast<size_t>(e->tdev.len - 7u) * 4u;
-  if (mode == kModeAdjoint) return static_cast<size_t>(e->tdev.time_bins + 1u) * 8u;
-  return 0;
+  const size_t pantry = static_cast<size_t>(e->cfg.block_size / 32) * kPantryBytesPerWarp;
+  if (mode == kModeTally && !batch) return pantry + static_cast<size_t>(e->tdev.len - 7u) * 4u;
+  if (mode == kModeAdjoint) return pantry + static_cast<size_t>(e->tdev.time_bins + 1u) * 8u;
+  return pantry;
+}
+
+// Register-budget variant of the wave kernel: 2, 3 or 4 blocks of 256 threads per SM.
+int engine_minb(const optx_engine* e) {
+  const int b = e->cfg.blocks_per_sm > 0 ? e->cfg.blocks_per_sm : 4;
+  return std::max(2, std::min(4, b));
 }
 
 int engine_grid(optx_engine* e, int mode, bool batch, int& grid) {
   const size_t smem = wave_smem(e, mode, batch);
   const int math = e->cfg.math;
-  if (smem > 48 * 1024) OPTX_CUDA(DISPATCH(math, wave_set_smem, mode, batch, smem));
-  int bps = DISPATCH(math, wave_blocks_per_sm, mode, batch, e->cfg.block_size, smem);
+  const int minb = engine_minb(e);
+  if (smem > 48 * 1024) OPTX_CUDA(DISPATCH(math, wave_set_smem, mode, batch, minb, smem));
+  int bps = DISPATCH(math, wave_blocks_per_sm, mode, batch, minb, e->cfg.block_size, smem);
   if (bps <= 0) return fail(OPTX_ERR_RUNTIME, "wavefront kernel cannot be resident with this block size / tally");
-  if (e->cfg.blocks_per_sm > 0) bps = std::min(bps, e->cfg.blocks_per_sm);
+  if (e->cfg.blocks_per_sm > 0) bps = std::min(bps, e->cfg.blocks_per_sm * (256 / e->cfg.block_size));
   grid = bps * e->n_sm;
   return OPTX_OK;
 }
@@ -317,6 +326,7 @@ int engine_upload_args(optx_engine* e, int mode, bool batch, int grid, cudaGraph
   std::memset(&a, 0, sizeof(a));
   a.params = e->d_params;
   a.offsets = e->d_offsets;
+  a.ev_table = e->d_evtable;
   a.n_events = e->n_events;
   a.threshold = e->cfg.threshold;
   a.cadence = e->cfg.cadence;
@@ -410,7 +420,7 @@ int engine_graph(optx_engine* e, int mode, bool batch, int grid, optx_engine::Gr
   DevParams p_copy = P0;
   void* wave_args[] = {&p_copy, &a_ptr, &c_ptr};
   cudaKernelNodeParams wp{};
-  wp.func = const_cast<void*>(DISPATCH(math, wave_kernel_fn, mode, batch));
+  wp.func = const_cast<void*>(DISPATCH(math, wave_kernel_fn, mode, batch, engine_minb(e)));
   wp.gridDim = dim3(grid);
   wp.blockDim = dim3(e->cfg.block_size);
   wp.sharedMemBytes = static_cast<unsigned>(smem);
@@ -448,8 +458,8 @@ int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_
                        std::max(1, std::min(grid, 4 * e->n_sm)), 256, st));
     const DevParams P0 = batch ? DevParams{} : e->P0;
     for (uint64_t w = 0;; ++w) {
-      OPTX_CUDA(DISPATCH(math, launch_wave, mode, batch, P0, e->d_args, e->d_ctrl, grid,
-                         e->cfg.block_size, smem, st));
+      OPTX_CUDA(DISPATCH(math, launch_wave, mode, batch, engine_minb(e), P0, e->d_args, e->d_ctrl,
+                         grid, e->cfg.block_size, smem, st));
       unsigned active = 0;
       OPTX_CUDA(cudaMemcpyAsync(&active, &e->d_ctrl->active, sizeof(active),
                                 cudaMemcpyDeviceToHost, st));
@@ -669,8 +679,9 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
   optx_wave_config k{};
   if (cfg) k = *cfg;
   if (k.block_size == 0) k.block_size = 256;
-  OPTX_TRY(check_block(k.block_size));
-  if (k.threshold == 0) k.threshold = 24;
+  if (k.block_size <= 0 || k.block_size % 32 != 0 || k.block_size > 256)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "wavefront block_size must be a multiple of 32 <= 256");
+  if (k.threshold == 0) k.threshold = 28;
   if (k.threshold > 32) return fail(OPTX_ERR_INVALID_ARGUMENT, "threshold must be 1..32");
   if (k.use_graph == 0) k.use_graph = 1;
   OPTX_TRY(check_math(k.math));
@@ -713,6 +724,7 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
       (rc = alloc(reinterpret_cast<void**>(&e->d_ctrl), sizeof(WaveCtrl))) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_params), sizeof(DevParams) * max_events)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_offsets), 8ull * (max_events + 1ull))) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_evtable), 4ull * ((max_photons >> kEvShift) + 2ull))) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_qa), qcap * 64ull)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_qb), qcap * 64ull)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_tally), 8ull * td.len * max_events)) ||
@@ -735,6 +747,7 @@ int optx_engine_destroy(optx_engine* e) {
   cudaFree(e->d_ctrl);
   cudaFree(e->d_params);
   cudaFree(e->d_offsets);
+  cudaFree(e->d_evtable);
   cudaFree(e->d_qa);
   cudaFree(e->d_qb);
   cudaFree(e->d_tally);
@@ -776,6 +789,8 @@ int optx_engine_set_events(optx_engine* e, const optx_params* events, const optx
                             cudaMemcpyHostToDevice, st));
   OPTX_CUDA(cudaMemcpyAsync(e->d_offsets, e->h_offsets.data(), 8ull * (n_events + 1ull),
                             cudaMemcpyHostToDevice, st));
+  if (n_events > 1 && total > 0)
+    OPTX_CUDA(DISPATCH(e->cfg.math, launch_event_table, e->d_offsets, n_events, e->d_evtable, total, st));
   return OPTX_OK;
 }
 
@@ -866,7 +881,7 @@ int optx_run_records_event(const optx_params* p, const optx_faces* faces, uint64
   const uint64_t cap = std::max<uint64_t>(1, std::min<uint64_t>({n, chunk ? chunk : (uint64_t{1} << 24), uint64_t{1} << 31}));
   optx_tally_config tc{1u, 1.0f, 1u};
   optx_wave_config cfg{};
-  cfg.block_size = block_size;
+  cfg.block_size = std::min(block_size, 256);  // launch geometry only; records do not depend on it
   cfg.threshold = 32;
   cfg.cadence = steps_per_launch >= p->max_steps ? 0u : steps_per_launch;
   cfg.use_graph = 1;

@@ -146,24 +146,28 @@ __global__ void history_tally_kernel(const DevParams P, const TallyDev tc, uint6
 // ---------------------------------------------------------------------------
 // Wavefront engine.
 
-__device__ __forceinline__ DevParams load_params(const DevParams* p) {
-  DevParams P;
-  const float4* src = reinterpret_cast<const float4*>(p);
-  float4* dst = reinterpret_cast<float4*>(&P);
-#pragma unroll
-  for (int i = 0; i < 7; ++i) dst[i] = __ldg(src + i);
-  return P;
+// Event of relative photon g: the table gives the event holding photon
+// (g >> kEvShift) << kEvShift; the scan moves past events that end before g
+// (one or two steps when events hold at least 128 photons).
+__device__ __forceinline__ uint32_t find_event(const WaveArgs* __restrict__ A, unsigned long long g) {
+  uint32_t e = __ldg(A->ev_table + (g >> kEvShift));
+  const unsigned long long* __restrict__ off = A->offsets;
+  while (e + 1u < A->n_events && __ldg(off + e + 1u) <= g) ++e;
+  return e;
 }
 
-// Largest e with offsets[e] <= g (offsets[0] = 0 <= g < offsets[n_events]).
-__device__ __forceinline__ uint32_t find_event(const unsigned long long* __restrict__ offsets,
-                                               uint32_t n_events, unsigned long long g) {
-  uint32_t lo = 0, hi = n_events;
-  while (hi - lo > 1u) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (__ldg(offsets + mid) <= g) lo = mid; else hi = mid;
-  }
-  return lo;
+// table[k] = the event that holds photon k << kEvShift (one thread per event).
+__global__ void event_table_kernel(const unsigned long long* __restrict__ offsets, uint32_t n_events,
+                                   uint32_t* __restrict__ table, unsigned long long total) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_events) return;
+  const unsigned long long lo = offsets[e], hi = offsets[e + 1] < total ? offsets[e + 1] : total;
+  for (unsigned long long k = (lo + (1ull << kEvShift) - 1ull) >> kEvShift; (k << kEvShift) < hi; ++k)
+    table[k] = e;
+}
+
+__device__ __forceinline__ float4 make_uint4_as_float4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  return make_float4(__uint_as_float(a), __uint_as_float(b), __uint_as_float(c), __uint_as_float(d));
 }
 
 // Queue slot -> first float4 of the photon in its 32-photon tile.
@@ -197,18 +201,32 @@ __global__ void wave_prep_kernel(const WaveArgs* __restrict__ A, WaveCtrl* __res
   }
 }
 
-template <int MODE, bool BATCH>
-__global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
-                                                   const WaveArgs* __restrict__ A,
-                                                   WaveCtrl* __restrict__ ctrl) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint32_t* s_hist = reinterpret_cast<uint32_t*>(smem_raw);  // tally, not batched
-  double* s_w = reinterpret_cast<double*>(smem_raw);         // adjoint weights
-  __shared__ double s_red[4][32];
+// Parameters of a lane's photon: the kernel argument (one configuration) or the
+// event's record in global memory, read field by field where the step uses it.
+template <bool BATCH>
+__device__ __forceinline__ const DevParams& params_of(const DevParams& P0,
+                                                      const WaveArgs* __restrict__ A, uint32_t ev) {
+  if (BATCH) return A->params[ev];
+  return P0;
+}
 
+// MINB: resident blocks of 256 threads per SM the register allocation must allow
+// (2: <= 128 registers, 3: <= 80, 4: <= 64); a tuning knob of the engine.
+template <int MODE, bool BATCH, int MINB>
+__global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
+                                                      const WaveArgs* __restrict__ A,
+                                                      WaveCtrl* __restrict__ ctrl) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t nwarps = blockDim.x >> 5;
+  // [pantries: nwarps x 32 x 112 B][block histograms (tally) or bin weights (adjoint)]
+  float4* pantry = reinterpret_cast<float4*>(smem_raw + warp * kPantryBytesPerWarp);
+  unsigned char* extra = smem_raw + nwarps * kPantryBytesPerWarp;
+  uint32_t* s_hist = reinterpret_cast<uint32_t*>(extra);
+  double* s_w = reinterpret_cast<double*>(extra);
+  __shared__ double s_red[4][16];
 
   const uint32_t wave = ctrl->wave;
   const uint32_t n_in = ctrl->n_in;
@@ -235,15 +253,16 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
   Rng r{};
   ScoreAux aux{0u, 0.0f};
   uint32_t pidx = 0u, ev = 0u;
-  bool alive = false, exhausted = false;
-  bool refilled = false;  // warp-uniform: lanes were loaded and have not stepped yet
+  bool alive = false;
+  bool exhausted = false;  // warp-uniform: the wave's work items are all handed out
+  bool refilled = false;   // warp-uniform: lanes were loaded and have not stepped yet
+  uint32_t pc = 0u;        // warp-uniform: photons waiting in this warp's pantry
   uint32_t wsteps = 0u;
   // Per-lane tallies (flushed at the end; batched: when the lane's event changes).
-  uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0;
-  unsigned long long snb = 0, sns = 0;
+  uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0, snb = 0, sns = 0;
   uint32_t cur_ev = 0xffffffffu;
   double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
-  unsigned long long useful = 0, issued = 0;
+  uint32_t useful = 0u, iters = 0u;
 
   auto flush_event = [&]() {
     if (cur_ev == 0xffffffffu) return;
@@ -253,10 +272,9 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
     if (f2) atomicAdd(&T0[2], static_cast<unsigned long long>(f2));
     if (f3) atomicAdd(&T0[3], static_cast<unsigned long long>(f3));
     if (f4) atomicAdd(&T0[4], static_cast<unsigned long long>(f4));
-    if (snb) atomicAdd(&T0[tc.len - 2u], snb);
-    if (sns) atomicAdd(&T0[tc.len - 1u], sns);
-    f0 = f1 = f2 = f3 = f4 = 0u;
-    snb = sns = 0ull;
+    if (snb) atomicAdd(&T0[tc.len - 2u], static_cast<unsigned long long>(snb));
+    if (sns) atomicAdd(&T0[tc.len - 1u], static_cast<unsigned long long>(sns));
+    f0 = f1 = f2 = f3 = f4 = snb = sns = 0u;
   };
 
   // Bookkeeping of a finished photon.
@@ -273,6 +291,17 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
       f2 += fate == 2u;
       f3 += fate == 3u;
       f4 += fate == 4u;
+      // Per-lane step sums stay far below 2^31 between flushes (a lane sees at
+      // most wave_quota / lanes photons of max_steps steps); flush early if not.
+      if (snb > 0x7fffffffu || sns > 0x7fffffffu) {
+        if (BATCH) {
+          flush_event();
+        } else {
+          atomicAdd(&A->tally[tc.len - 2u], static_cast<unsigned long long>(snb));
+          atomicAdd(&A->tally[tc.len - 1u], static_cast<unsigned long long>(sns));
+          snb = sns = 0u;
+        }
+      }
       snb += s.nb;
       sns += s.ns;
       if (fate == kDetected) {
@@ -330,53 +359,99 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
       break;
     }
     uint32_t amask = __ballot_sync(kFull, alive);
-    if (static_cast<uint32_t>(__popc(amask)) < T) {
-      if (!exhausted) {
-        const uint32_t need = 32u - static_cast<uint32_t>(__popc(amask));
+    uint32_t na = static_cast<uint32_t>(__popc(amask));
+    if (na < T) {
+      const uint32_t need = 32u - na;
+      if (pc < need && !exhausted) {
+        // Refill the pantry: all lanes emit (or load) one photon each together,
+        // so emission code runs on full warps.
+        const uint32_t room = 32u - pc;
         uint32_t base = 0u;
-        if (lane == 0u) base = atomicAdd(&ctrl->cursor, need);
+        if (lane == 0u) base = atomicAdd(&ctrl->cursor, room);
         base = __shfl_sync(kFull, base, 0);
-        const uint32_t got = base >= items ? 0u : min(need, items - base);
-        exhausted = got < need;
-        refilled = got > 0u;
-        const uint32_t rank = static_cast<uint32_t>(__popc(~amask & lt));
-        if (!alive && rank < got) {
-          const uint32_t item = base + rank;
+        const uint32_t got = base >= items ? 0u : min(room, items - base);
+        exhausted = got < room;
+        if (lane < got) {
+          const uint32_t item = base + lane;
+          Photon ns{};
+          Rng nr{};
+          ScoreAux na_aux{0u, 0.0f};
+          uint32_t npidx, nev = 0u;
           if (item < n_in) {
             // A survivor of the previous wave: 4 x 128-bit loads from its tile.
             const float4* q = qin + qidx(item);
             const float4 a = q[0], b = q[32], c = q[64], d = q[96];
-            s.px = a.x; s.py = a.y; s.pz = a.z; s.t = a.w;
-            s.dx = b.x; s.dy = b.y; s.dz = b.z; s.path = b.w;
-            s.nb = __float_as_uint(c.x);
-            s.ns = __float_as_uint(c.y);
-            pidx = __float_as_uint(c.w);
-            aux.n_refl = __float_as_uint(d.x);
-            aux.t_emit = d.y;
-            ev = __float_as_uint(d.z);
-            const DevParams P = BATCH ? load_params(A->params + ev) : P0;
-            r.init(first_id + pidx, P.key_lo, P.key_hi, __float_as_uint(c.z));
-            alive = true;
+            ns.px = a.x; ns.py = a.y; ns.pz = a.z; ns.t = a.w;
+            ns.dx = b.x; ns.dy = b.y; ns.dz = b.z; ns.path = b.w;
+            ns.nb = __float_as_uint(c.x);
+            ns.ns = __float_as_uint(c.y);
+            npidx = __float_as_uint(c.w);
+            na_aux.n_refl = __float_as_uint(d.x);
+            na_aux.t_emit = d.y;
+            nev = __float_as_uint(d.z);
+            const DevParams& P = params_of<BATCH>(P0, A, nev);
+            nr.init(first_id + npidx, P.key_lo, P.key_hi, __float_as_uint(c.z));
           } else {
             const unsigned long long g = fresh_next + (item - n_in);
-            pidx = static_cast<uint32_t>(g);
-            if (BATCH) ev = find_event(A->offsets, A->n_events, g);
-            const DevParams P = BATCH ? load_params(A->params + ev) : P0;
-            r.init(first_id + g, P.key_lo, P.key_hi, 0u);
-            aux.n_refl = 0u;
-            start_photon<MODE == kModeAdjoint>(P, s, r, aux);
-            alive = P.max_steps > 0u;
-            if (!alive) finish(kMaxSteps, P);
+            npidx = static_cast<uint32_t>(g);
+            if (BATCH) nev = find_event(A, g);
+            const DevParams& P = params_of<BATCH>(P0, A, nev);
+            nr.init(first_id + g, P.key_lo, P.key_hi, 0u);
+            start_photon<MODE == kModeAdjoint>(P, ns, nr, na_aux);
           }
-          wsteps = 0u;
+          float4* e = pantry + (pc + lane) * 7u;
+          e[0] = make_float4(ns.px, ns.py, ns.pz, ns.t);
+          e[1] = make_float4(ns.dx, ns.dy, ns.dz, ns.path);
+          e[2] = make_uint4_as_float4(ns.nb, ns.ns, npidx, nev);
+          e[3] = make_uint4_as_float4(nr.w[0], nr.w[1], nr.w[2], nr.w[3]);
+          e[4] = make_uint4_as_float4(nr.w[4], nr.w[5], nr.w[6], nr.w[7]);
+          e[5] = make_float4(__uint_as_float(nr.o), __uint_as_float(nr.blk),
+                             __uint_as_float(na_aux.n_refl), na_aux.t_emit);
         }
-        amask = __ballot_sync(kFull, alive);
+        pc += got;
+        __syncwarp();
       }
-      if (exhausted) {
-        const uint32_t na = static_cast<uint32_t>(__popc(amask));
+      if (pc > 0u) {
+        // Idle lanes take photons from the top of the pantry.
+        const uint32_t take = min(need, pc);
+        const uint32_t rank = static_cast<uint32_t>(__popc(~amask & lt));
+        if (!alive && rank < take) {
+          const float4* e = pantry + (pc - 1u - rank) * 7u;
+          const float4 a = e[0], b = e[1], c = e[2], d = e[3], f = e[4], h = e[5];
+          s.px = a.x; s.py = a.y; s.pz = a.z; s.t = a.w;
+          s.dx = b.x; s.dy = b.y; s.dz = b.z; s.path = b.w;
+          s.nb = __float_as_uint(c.x);
+          s.ns = __float_as_uint(c.y);
+          pidx = __float_as_uint(c.z);
+          ev = __float_as_uint(c.w);
+          r.w[0] = __float_as_uint(d.x); r.w[1] = __float_as_uint(d.y);
+          r.w[2] = __float_as_uint(d.z); r.w[3] = __float_as_uint(d.w);
+          r.w[4] = __float_as_uint(f.x); r.w[5] = __float_as_uint(f.y);
+          r.w[6] = __float_as_uint(f.z); r.w[7] = __float_as_uint(f.w);
+          r.o = __float_as_uint(h.x);
+          r.blk = __float_as_uint(h.y);
+          aux.n_refl = __float_as_uint(h.z);
+          aux.t_emit = h.w;
+          const DevParams& P = params_of<BATCH>(P0, A, ev);
+          const unsigned long long id = first_id + pidx;
+          r.id_lo = static_cast<uint32_t>(id);
+          r.id_hi = static_cast<uint32_t>(id >> 32);
+          r.k0 = P.key_lo;
+          r.k1 = P.key_hi;
+          wsteps = 0u;
+          alive = s.nb + s.ns < P.max_steps;
+          if (!alive) finish(kMaxSteps, P);
+        }
+        pc -= take;
+        refilled = true;
+        __syncwarp();
+        amask = __ballot_sync(kFull, alive);
+        na = static_cast<uint32_t>(__popc(amask));
+      }
+      if (exhausted && pc == 0u) {
         if (na == 0u) break;
-        // Spill only photons that have stepped in this wave, so that every
-        // item of a wave makes progress and the run always ends.
+        // Spill only photons that have stepped in this wave, so that every item
+        // of a wave makes progress and the run always ends.
         if (na < T && !refilled) {
           spill_lanes(alive);
           alive = false;
@@ -387,7 +462,7 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
 
     // One step for every live lane.
     if (alive) {
-      const DevParams P = BATCH ? load_params(A->params + ev) : P0;
+      const DevParams& P = params_of<BATCH>(P0, A, ev);
       uint32_t fate = kMaxSteps;
       const bool still = step_photon<MODE == kModeAdjoint>(P, s, r, fate, aux);
       ++wsteps;
@@ -400,8 +475,8 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
       }
     }
     refilled = false;
-    issued += 32u;
-    useful += static_cast<uint32_t>(__popc(amask));
+    ++iters;
+    useful += na;
     if (cadence != 0u) {  // forced compaction after `cadence` steps in this wave
       const bool sp = alive && wsteps >= cadence;
       spill_lanes(sp);
@@ -411,8 +486,8 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
 
   // ---- end of this block's share of the wave: flush --------------------------
   if (lane == 0u) {
-    atomicAdd(&ctrl->useful, useful);
-    atomicAdd(&ctrl->issued, issued);
+    atomicAdd(&ctrl->useful, static_cast<unsigned long long>(useful));
+    atomicAdd(&ctrl->issued, 32ull * iters);
   }
   if (MODE == kModeTally) {
     if (BATCH) {
@@ -452,8 +527,7 @@ __global__ void __launch_bounds__(512) wave_kernel(const DevParams P0,
     __syncthreads();
     if (threadIdx.x < 4u) {
       double acc = 0.0;
-      const uint32_t nw = blockDim.x >> 5;
-      for (uint32_t w = 0; w < nw; ++w) acc += s_red[threadIdx.x][w];
+      for (uint32_t w = 0; w < nwarps; ++w) acc += s_red[threadIdx.x][w];
       if (acc != 0.0) atomicAdd(&A->grad[threadIdx.x], acc);
     }
   }
@@ -534,35 +608,45 @@ cudaError_t launch_wave_prep(const WaveArgs* A_dev, WaveCtrl* ctrl, int grid, in
 }
 
 template <int MODE, bool BATCH>
-static const void* kfn() {
-  return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH>);
-}
-
-const void* wave_kernel_fn(int mode, bool batch) {
-  switch (mode) {
-    case kModeTally: return batch ? kfn<kModeTally, true>() : kfn<kModeTally, false>();
-    case kModeRecords: return batch ? kfn<kModeRecords, true>() : kfn<kModeRecords, false>();
-    default: return batch ? kfn<kModeAdjoint, true>() : kfn<kModeAdjoint, false>();
+static const void* kfn(int minb) {
+  switch (minb) {
+    case 3: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 3>);
+    case 4: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 4>);
+    default: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 2>);
   }
 }
 
-int wave_blocks_per_sm(int mode, bool batch, int block, size_t smem) {
+const void* wave_kernel_fn(int mode, bool batch, int minb) {
+  switch (mode) {
+    case kModeTally: return batch ? kfn<kModeTally, true>(minb) : kfn<kModeTally, false>(minb);
+    case kModeRecords: return batch ? kfn<kModeRecords, true>(minb) : kfn<kModeRecords, false>(minb);
+    default: return batch ? kfn<kModeAdjoint, true>(minb) : kfn<kModeAdjoint, false>(minb);
+  }
+}
+
+int wave_blocks_per_sm(int mode, bool batch, int minb, int block, size_t smem) {
   int b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, wave_kernel_fn(mode, batch), block, smem) !=
-      cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, wave_kernel_fn(mode, batch, minb), block,
+                                                    smem) != cudaSuccess)
     return 0;
   return b;
 }
 
-cudaError_t wave_set_smem(int mode, bool batch, size_t smem) {
-  return cudaFuncSetAttribute(wave_kernel_fn(mode, batch),
+cudaError_t wave_set_smem(int mode, bool batch, int minb, size_t smem) {
+  return cudaFuncSetAttribute(wave_kernel_fn(mode, batch, minb),
                               cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
 }
 
-cudaError_t launch_wave(int mode, bool batch, const DevParams& P, const WaveArgs* A_dev,
+cudaError_t launch_wave(int mode, bool batch, int minb, const DevParams& P, const WaveArgs* A_dev,
                         WaveCtrl* ctrl, int grid, int block, size_t smem, cudaStream_t st) {
   void* args[] = {const_cast<DevParams*>(&P), &A_dev, &ctrl};
-  return cudaLaunchKernel(wave_kernel_fn(mode, batch), dim3(grid), dim3(block), args, smem, st);
+  return cudaLaunchKernel(wave_kernel_fn(mode, batch, minb), dim3(grid), dim3(block), args, smem, st);
+}
+
+cudaError_t launch_event_table(const unsigned long long* offsets, uint32_t n_events,
+                               uint32_t* table, unsigned long long total, cudaStream_t st) {
+  event_table_kernel<<<(n_events + 255) / 256, 256, 0, st>>>(offsets, n_events, table, total);
+  return cudaGetLastError();
 }
 
 }  // namespace OPTX_NS

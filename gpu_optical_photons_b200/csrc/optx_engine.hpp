@@ -24,6 +24,7 @@ struct TallyDev {
 struct WaveArgs {
   const DevParams* params;              // event table (1 entry when not batched)
   const unsigned long long* offsets;    // n_events + 1 relative photon offsets (batched)
+  const uint32_t* ev_table;             // event of photon (k << kEvShift), k < total >> kEvShift + 1
   uint32_t n_events;
   uint32_t threshold;                   // refill a warp when fewer lanes than this are alive (1..32)
   uint32_t cadence;                     // steps per photon per wave before a forced spill (0 = none)
@@ -66,6 +67,10 @@ struct WaveCtrl {
 };
 
 enum WaveMode : int { kModeTally = 0, kModeRecords = 1, kModeAdjoint = 2 };
+constexpr uint32_t kEvShift = 7;  // event lookup table: one entry per 128 photons
+// Shared memory of one warp's pantry: 32 ready photons x 112 bytes (7 x 16 B;
+// the 112-byte stride makes 8 lanes' 128-bit accesses hit 8 distinct bank groups).
+constexpr uint32_t kPantryBytesPerWarp = 32u * 112u;
 constexpr unsigned kErrQueue = 1u, kErrWatchdog = 2u;
 
 #define OPTX_DECLARE_LAUNCHERS(NS)                                                               \
@@ -80,11 +85,14 @@ constexpr unsigned kErrQueue = 1u, kErrWatchdog = 2u;
   cudaError_t launch_wave_prep(const WaveArgs* A_dev, WaveCtrl* ctrl, int grid, int block,       \
                                cudaStream_t st);                                                 \
   const void* wave_prep_fn();                                                                    \
-  const void* wave_kernel_fn(int mode, bool batch);                                              \
-  int wave_blocks_per_sm(int mode, bool batch, int block, size_t smem);                          \
-  cudaError_t wave_set_smem(int mode, bool batch, size_t smem);                                  \
-  cudaError_t launch_wave(int mode, bool batch, const DevParams& P, const WaveArgs* A_dev,        \
-                          WaveCtrl* ctrl, int grid, int block, size_t smem, cudaStream_t st);    \
+  const void* wave_kernel_fn(int mode, bool batch, int minb);                                    \
+  int wave_blocks_per_sm(int mode, bool batch, int minb, int block, size_t smem);                \
+  cudaError_t wave_set_smem(int mode, bool batch, int minb, size_t smem);                        \
+  cudaError_t launch_wave(int mode, bool batch, int minb, const DevParams& P,                    \
+                          const WaveArgs* A_dev, WaveCtrl* ctrl, int grid, int block,            \
+                          size_t smem, cudaStream_t st);                                         \
+  cudaError_t launch_event_table(const unsigned long long* offsets, uint32_t n_events,           \
+                                 uint32_t* table, unsigned long long total, cudaStream_t st);    \
   }
 
 OPTX_DECLARE_LAUNCHERS(fast)

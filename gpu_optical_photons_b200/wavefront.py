@@ -22,8 +22,8 @@ from .backend import Tally, _stream_ptr, _crec_from_torch
 @dataclass
 class WaveConfig:
     block_size: int = 256
-    blocks_per_sm: int = 0      # 0 = occupancy limit
-    threshold: int = 24         # refill when fewer lanes than this are alive
+    blocks_per_sm: int = 0      # resident 256-thread blocks per SM (2/3/4 = register budget); 0 = 4
+    threshold: int = 28         # refill when fewer lanes than this are alive
     cadence: int = 0            # forced spill after this many steps per wave (0 = off)
     wave_quota: int = 0         # fresh photons per wave (0 = all)
     use_graph: bool = True

@@ -91,9 +91,10 @@ typedef struct optx_event_stats {
 
 /* Wavefront engine configuration. Zero fields take defaults. */
 typedef struct optx_wave_config {
-  int32_t block_size;    /* threads per block, multiple of 32 (default 256) */
-  int32_t blocks_per_sm; /* persistent grid = blocks_per_sm x SMs (0: occupancy limit) */
-  uint32_t threshold;    /* refill a warp when fewer than this many lanes are alive, 1..32 (default 24) */
+  int32_t block_size;    /* threads per block, multiple of 32, <= 256 (default 256) */
+  int32_t blocks_per_sm; /* resident 256-thread blocks per SM: 2, 3 or 4 (register budget
+                            <= 128 / 80 / 64); the persistent grid is that x SMs (default 4) */
+  uint32_t threshold;    /* refill a warp when fewer than this many lanes are alive, 1..32 (default 28) */
   uint32_t cadence;      /* steps per photon per wave before a forced spill, 0 = none (default 0) */
   uint64_t wave_quota;   /* fresh photons admitted per wave, 0 = all (default) */
   int32_t use_graph;     /* 1: waves run as a CUDA-graph while loop (default); -1: host loop */
