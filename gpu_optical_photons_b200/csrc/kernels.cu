@@ -332,12 +332,16 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
   };
 
   // Warp-collective: spill the lanes with `spill` set into the output queue.
-  auto spill_lanes = [&](bool spill) {
+  // Returns true for the lanes whose photon went to the queue; when the queue
+  // is full the others keep their photon (the capacity only limits compaction).
+  bool queue_full = false;  // warp-uniform
+  auto spill_lanes = [&](bool spill) -> bool {
     const uint32_t smask = __ballot_sync(kFull, spill);
-    if (smask == 0u) return;
+    if (smask == 0u) return false;
     uint32_t base = 0u;
     if (lane == 0u) base = atomicAdd(&ctrl->n_out, static_cast<unsigned>(__popc(smask)));
     base = __shfl_sync(kFull, base, 0);
+    bool done = false;
     if (spill) {
       const uint32_t slot = base + static_cast<uint32_t>(__popc(smask & lt));
       if (slot < qcap) {
@@ -347,10 +351,11 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
         q[64] = make_float4(__uint_as_float(s.nb), __uint_as_float(s.ns),
                             __uint_as_float(r.draws()), __uint_as_float(pidx));
         q[96] = make_float4(__uint_as_float(aux.n_refl), aux.t_emit, __uint_as_float(ev), 0.0f);
-      } else {
-        atomicOr(&ctrl->error, kErrQueue);
+        done = true;
       }
     }
+    if (__ballot_sync(kFull, spill && !done) != 0u) queue_full = true;
+    return done;
   };
 
   for (unsigned long long it = 0;; ++it) {
@@ -452,10 +457,9 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
         if (na == 0u) break;
         // Spill only photons that have stepped in this wave, so that every item
         // of a wave makes progress and the run always ends.
-        if (na < T && !refilled) {
-          spill_lanes(alive);
-          alive = false;
-          break;
+        if (na < T && !refilled && !queue_full) {
+          if (spill_lanes(alive)) alive = false;
+          if (__ballot_sync(kFull, alive) == 0u) break;
         }
       }
     }
@@ -477,10 +481,8 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
     refilled = false;
     ++iters;
     useful += na;
-    if (cadence != 0u) {  // forced compaction after `cadence` steps in this wave
-      const bool sp = alive && wsteps >= cadence;
-      spill_lanes(sp);
-      if (sp) alive = false;
+    if (cadence != 0u && !queue_full) {  // forced compaction after `cadence` steps in this wave
+      if (spill_lanes(alive && wsteps >= cadence)) alive = false;
     }
   }
 
@@ -540,7 +542,7 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
     if (done == gridDim.x - 1u) {
       __threadfence();
       volatile WaveCtrl* vc = ctrl;
-      const unsigned n_out = vc->n_out;
+      const unsigned n_out = vc->n_out < qcap ? vc->n_out : qcap;  // reservations past qcap were not written
       const unsigned long long next = vc->fresh_next + vc->fresh_count;
       const unsigned long long remaining = A->total - next;
       unsigned long long fresh = remaining < A->wave_quota ? remaining : A->wave_quota;
