@@ -926,3 +926,117 @@ int optx_run_records_event(const optx_params* p, const optx_faces* faces, uint64
 }
 
 }  // extern "C"
+
+// =============================================================================
+// Wavefront tally without device allocation.
+//
+// For callers that cannot call cudaMalloc: code running where another runtime
+// or framework owns the device memory (a caching allocator that must see every
+// allocation, a memory-capped process, a plugin that may not grow its footprint
+// after start-up). All of the run's device scratch lives in the file-scope
+// array below, which the library holds on every GPU that loads it, until exit.
+namespace {
+
+constexpr uint32_t kNoAllocQueuePhotons = 16384;  // per state queue (64 B per photon)
+constexpr uint32_t kNoAllocMaxTally = 65536;      // max tally length (u64 entries)
+constexpr size_t kNoAllocArgsOff = 0;
+constexpr size_t kNoAllocCtrlOff = 1024;
+constexpr size_t kNoAllocTallyOff = 2048;
+constexpr size_t kNoAllocQaOff = kNoAllocTallyOff + 8ull * kNoAllocMaxTally;
+constexpr size_t kNoAllocQbOff = kNoAllocQaOff + 64ull * kNoAllocQueuePhotons;
+constexpr size_t kNoAllocScratchBytes = kNoAllocQbOff + 64ull * kNoAllocQueuePhotons;  // 2.6 MiB
+static_assert(sizeof(WaveArgs) <= kNoAllocCtrlOff && sizeof(WaveCtrl) <= kNoAllocTallyOff - kNoAllocCtrlOff,
+              "no-alloc scratch layout");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};  // device address of the array, per device
+
+}  // namespace
+
+extern "C" int optx_wavefront_tally_noalloc(const optx_params* p, const optx_faces* faces,
+                                            const optx_tally_config* c, uint64_t n,
+                                            uint64_t first_id, uint64_t* tally_out, int math,
+                                            void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  OPTX_TRY(check_params(p, faces));
+  OPTX_TRY(check_math(math));
+  TallyDev td{};
+  OPTX_TRY(make_tally_dev(c, td));
+  if (td.len > kNoAllocMaxTally)
+    return fail(OPTX_ERR_INVALID_ARGUMENT,
+                "optx_wavefront_tally_noalloc: tally length " + std::to_string(td.len) +
+                    " exceeds the static scratch maximum of " + std::to_string(kNoAllocMaxTally) +
+                    " entries (5 + time_bins + 1 + xy_bins^2 + 2)");
+  if (n > 0xffffffffull)
+    return fail(OPTX_ERR_INVALID_ARGUMENT,
+                "optx_wavefront_tally_noalloc: at most 2^32 - 1 photons per call");
+  if (tally_out == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "tally_out must not be NULL");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(OPTX_ERR_NO_DEVICE, "no CUDA device available");
+  }
+  int dev = 0;
+  OPTX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(OPTX_ERR_RUNTIME, "device ordinal out of range");
+  // First call on this device: the host-side name of the array is not a device
+  // address, so look the address up once (with this device current).
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void* ptr = nullptr;
+    OPTX_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = ptr;
+  }
+  unsigned char* base = static_cast<unsigned char*>(g_noalloc_ptr[dev]);
+  auto* d_args = reinterpret_cast<WaveArgs*>(base + kNoAllocArgsOff);
+  auto* d_ctrl = reinterpret_cast<WaveCtrl*>(base + kNoAllocCtrlOff);
+  auto* d_tally = reinterpret_cast<unsigned long long*>(base + kNoAllocTallyOff);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+  const DevParams P = make_dev_params(*p, faces);
+  constexpr int kBlock = 256, kMinB = 4;
+  const size_t smem = static_cast<size_t>(kBlock / 32) * kPantryBytesPerWarp +
+                      static_cast<size_t>(td.len - 7u) * 4u;
+  if (smem > 48 * 1024) OPTX_CUDA(DISPATCH(math, wave_set_smem, kModeTally, false, kMinB, smem));
+  const int bps = DISPATCH(math, wave_blocks_per_sm, kModeTally, false, kMinB, kBlock, smem);
+  if (bps <= 0)
+    return fail(OPTX_ERR_RUNTIME, "tally histograms need too much shared memory; reduce xy_bins / time_bins");
+  const int grid = std::min(bps, kMinB) * num_sms();
+
+  WaveArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n_events = 1;
+  a.threshold = 28;
+  a.cadence = 0;
+  a.qcap = kNoAllocQueuePhotons;
+  a.total = n;
+  a.first_id = first_id;
+  a.wave_quota = 1ull << 30;
+  a.qa = reinterpret_cast<float4*>(base + kNoAllocQaOff);
+  a.qb = reinterpret_cast<float4*>(base + kNoAllocQbOff);
+  a.tally = d_tally;
+  a.tc = td;
+  a.use_graph = 0u;
+  a.iter_cap = (static_cast<unsigned long long>(n) + a.qcap + 64ull) * (P.max_steps + 2ull) + 4096ull;
+  a.wave_cap = static_cast<uint32_t>(std::min<unsigned long long>(
+      std::max<unsigned long long>(4ull * (P.max_steps + 2ull) + 64ull, 100000ull), 0xfffffff0ull));
+  OPTX_CUDA(cudaMemcpyAsync(d_args, &a, sizeof(a), cudaMemcpyHostToDevice, st));
+  // The prep kernel clears what must start at zero: the control block and the
+  // tally accumulator (the array keeps the previous call's contents).
+  OPTX_CUDA(DISPATCH(math, launch_wave_prep, d_args, d_ctrl, std::min(grid, 4 * num_sms()), 256, st));
+  for (;;) {
+    OPTX_CUDA(DISPATCH(math, launch_wave, kModeTally, false, kMinB, P, d_args, d_ctrl, grid, kBlock,
+                       smem, st));
+    unsigned active = 0;
+    OPTX_CUDA(cudaMemcpyAsync(&active, &d_ctrl->active, sizeof(active), cudaMemcpyDeviceToHost, st));
+    OPTX_CUDA(cudaStreamSynchronize(st));
+    if (!active) break;  // the kernel ends the run itself at its wave cap
+  }
+  unsigned error = 0;
+  OPTX_CUDA(cudaMemcpyAsync(&error, &d_ctrl->error, sizeof(error), cudaMemcpyDeviceToHost, st));
+  OPTX_CUDA(cudaMemcpyAsync(tally_out, d_tally, 8ull * td.len, cudaMemcpyDeviceToHost, st));
+  OPTX_CUDA(cudaStreamSynchronize(st));
+  if (error & kErrWatchdog) return fail(OPTX_ERR_WATCHDOG, "wavefront iteration cap reached");
+  return OPTX_OK;
+}

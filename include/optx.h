@@ -180,6 +180,24 @@ int optx_run_batch(optx_engine* e, const optx_params* events, const optx_faces* 
                    const uint64_t* counts, uint32_t n_events, uint64_t first_id,
                    uint64_t* host_tallies, optx_event_stats* stats, optx_timing* timing);
 
+/* ---- wavefront tally without device allocation -------------------------- */
+/* No counterpart in the reference. For callers that cannot call cudaMalloc
+ * (the device memory belongs to another runtime or framework allocator, or the
+ * process may not grow its device footprint after start-up): the same result as
+ * optx_run_tally (the wavefront engine on one configuration, host output), with
+ * all device scratch in a static 2.6 MiB array of the library that every GPU
+ * loading liboptx.so holds until the process exits. It calls no cudaMalloc,
+ * cudaFree or other allocating routine. Limits: tally length (5 + time_bins + 1 +
+ * xy_bins^2 + 2) <= 65536 entries and n < 2^32; larger requests fail with
+ * OPTX_ERR_INVALID_ARGUMENT. The first call on a device looks up the array's
+ * device address (make that first call before any stream capture). Every call
+ * shares the one array: calls that overlap on the GPU (other streams or host
+ * threads) race; the library serialises calls from one process. Synchronous on
+ * `stream`; tally_out is a host array, overwritten. */
+int optx_wavefront_tally_noalloc(const optx_params* p, const optx_faces* faces,
+                                 const optx_tally_config* c, uint64_t n, uint64_t first_id,
+                                 uint64_t* tally_out, int math, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
