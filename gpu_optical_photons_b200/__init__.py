@@ -16,4 +16,13 @@ from .backend import (Records, Tally, gpu_available, gpu_device_name, run_gpu_re
                       device_records, records_to_numpy)
 from .wavefront import WavefrontEngine, WaveConfig, wavefront_tally, batched_events
 
+
+def __getattr__(name):
+    # The differentiable response needs torch; import it on first use.
+    if name in ("ResponseModel", "response", "loss_fn", "nll_loss", "calibrate", "crn_central_fd",
+                "target_histogram"):
+        from . import adjoint
+        return getattr(adjoint, name)
+    raise AttributeError(name)
+
 __all__ = [n for n in dir() if not n.startswith("_")]

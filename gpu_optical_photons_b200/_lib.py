@@ -87,6 +87,8 @@ _SIGS = {
     "optx_engine_set_events": [_P, _P, _P, _P, ctypes.c_uint32, _u64, _P],
     "optx_engine_run_tally": [_P, _P],
     "optx_engine_run_records": [_P, _P, _P],
+    "optx_engine_run_adjoint": [_P, _P, ctypes.c_double, _P, _P],
+    "optx_wavefront_tally_noalloc": [_P, _P, _P, _u64, _u64, _P, _int, _P],
     "optx_engine_tally_ptr": [_P, _P, _P],
     "optx_engine_get_tallies": [_P, _P, _P],
     "optx_engine_stats": [_P, _P, _P],

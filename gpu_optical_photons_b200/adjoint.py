@@ -1,0 +1,197 @@
+"""Differentiable detector response: a torch.autograd.Function over the C ABI.
+
+Forward: the wavefront engine tallies N photons at theta = (abs_length,
+scat_length, reflectivity, tau) and returns the arrival-time histogram h
+(time_bins + 1 counts, last = overflow) and the detected fraction D.
+
+Backward: ``optx_engine_run_adjoint`` replays the same photons from their
+Philox counters (no stored paths) and accumulates, in FP64, the score-function
+(likelihood-ratio) estimator of d E[h_b] / d theta weighted by the incoming
+gradients. For a photon history with path length s, n_s scatterings, k
+reflections at painted faces and emission time t_e, the score of its
+probability density is
+
+    S_La  = s / La^2 - [absorbed in bulk] / La
+    S_Ls  = s / Ls^2 - n_s / Ls
+    S_R   = k / R - [absorbed at a painted face] / (1 - R)
+    S_tau = t_e / tau^2 - 1 / tau
+
+(exponential free paths of mean La, Ls; Bernoulli reflection with probability
+R; exponential emission time). Only detected photons enter the histogram, so
+the absorbed-photon terms drop out. d E[h_b] / d theta = E[1_b S] and the
+estimate sum_photons 1_b S is unbiased; it is checked against common-random-
+number central finite differences and the oracle's FP64 CPU gradient.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .params import SimParams, TallyConfig
+from .wavefront import WaveConfig, WavefrontEngine
+
+THETA_NAMES = ("abs_length", "scat_length", "reflectivity", "tau")
+
+
+def with_theta(p: SimParams, theta) -> SimParams:
+    t = [float(np.float32(v)) for v in theta]
+    return p.replace(abs_length=t[0], scat_length=t[1], reflectivity=t[2], tau=t[3])
+
+
+class ResponseModel:
+    """Owns a single-configuration wavefront engine for forward and replay runs."""
+
+    def __init__(self, base: SimParams, n: int, tally: TallyConfig | None = None, first_id: int = 0,
+                 config: WaveConfig | None = None):
+        self.base = base
+        self.n = n
+        self.first_id = first_id
+        self.tally = tally or TallyConfig(500, 50.0, 1)
+        self.engine = WavefrontEngine(self.tally, 1, n, config or WaveConfig())
+        self._theta = None
+
+    def _upload(self, theta):
+        key = tuple(float(np.float32(v)) for v in theta)
+        if key != self._theta:
+            self.engine.set_events([with_theta(self.base, key)], [self.n], self.first_id)
+            self._theta = key
+
+    def forward(self, theta) -> tuple[np.ndarray, int]:
+        """(arrival-time histogram incl. overflow, detected count) at theta."""
+        self._upload(theta)
+        self.engine.run_tally()
+        flat = self.engine.tallies()[0]
+        tb = self.tally.time_bins
+        return flat[5:5 + tb + 1].astype(np.float64), int(flat[0])
+
+    def replay(self, theta, w_bin: torch.Tensor, w_det: float) -> np.ndarray:
+        """FP64 sum over detected photons of (w_bin[bin] + w_det) * score."""
+        self._upload(theta)
+        w = w_bin.detach().to(device="cuda", dtype=torch.float64).contiguous()
+        assert w.numel() == self.tally.time_bins + 1
+        grad = torch.zeros(4, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        _lib.call("optx_engine_run_adjoint", self.engine._h, ctypes.c_void_p(w.data_ptr()),
+                  float(w_det), ctypes.c_void_p(grad.data_ptr()), ctypes.c_void_p(stream))
+        return grad.cpu().numpy()
+
+    def close(self):
+        self.engine.close()
+
+
+class _Response(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, theta: torch.Tensor, model: ResponseModel):
+        th = theta.detach().cpu().numpy().astype(np.float64)
+        hist, det = model.forward(th)
+        ctx.model = model
+        ctx.theta = th
+        return (torch.as_tensor(hist, dtype=torch.float64, device=theta.device),
+                torch.tensor(det / model.n, dtype=torch.float64, device=theta.device))
+
+    @staticmethod
+    def backward(ctx, grad_hist, grad_det):
+        model = ctx.model
+        w_bin = grad_hist if grad_hist is not None else torch.zeros(model.tally.time_bins + 1)
+        w_det = float(grad_det) / model.n if grad_det is not None else 0.0
+        g = model.replay(ctx.theta, w_bin, w_det)
+        return torch.as_tensor(g, dtype=torch.float64), None
+
+
+def response(theta: torch.Tensor, model: ResponseModel):
+    """(histogram h, detected fraction D) as differentiable functions of theta (4,)."""
+    return _Response.apply(theta, model)
+
+
+def poisson_nll(hist: torch.Tensor, target: torch.Tensor, n: int, bins: int) -> torch.Tensor:
+    """Poisson negative log-likelihood of the first `bins` bins, per photon.
+
+    lambda_b = h_b + 1 (one pseudo-count keeps log finite in empty bins)."""
+    lam = hist[:bins] + 1.0
+    k = target[:bins]
+    return (lam - k * torch.log(lam)).sum() / n
+
+
+def loss_fn(theta: torch.Tensor, model: ResponseModel, target: torch.Tensor) -> torch.Tensor:
+    """The calibration loss: Poisson NLL of the arrival-time histogram plus D."""
+    h, d = response(theta, model)
+    return poisson_nll(h, target, model.n, model.tally.time_bins) + d
+
+
+def loss_value(theta, model: ResponseModel, target: np.ndarray) -> float:
+    hist, det = model.forward(theta)
+    lam = hist[:model.tally.time_bins] + 1.0
+    k = target[:model.tally.time_bins]
+    return float((lam - k * np.log(lam)).sum() / model.n + det / model.n)
+
+
+def crn_central_fd(theta, model: ResponseModel, target: np.ndarray, rel_step: float = 1e-3):
+    """Central finite differences with common random numbers (same photons / seed).
+
+    The step is rel_step * theta_j rounded to the float32 grid; the divisor is the
+    actual difference of the float32 parameters."""
+    theta = np.asarray(theta, np.float64)
+    g = np.zeros(4)
+    for j in range(4):
+        up, dn = theta.copy(), theta.copy()
+        up[j] = float(np.float32(theta[j] * (1 + rel_step)))
+        dn[j] = float(np.float32(theta[j] * (1 - rel_step)))
+        g[j] = (loss_value(up, model, target) - loss_value(dn, model, target)) / (up[j] - dn[j])
+    return g
+
+
+def target_histogram(base: SimParams, theta_target, n: int, seed: int = 777,
+                     tally: TallyConfig | None = None) -> np.ndarray:
+    """Arrival-time histogram of a run at theta_target with its own seed."""
+    m = ResponseModel(base.replace(seed=seed), n, tally)
+    try:
+        hist, _ = m.forward(theta_target)
+    finally:
+        m.close()
+    return hist
+
+
+def nll_loss(theta: torch.Tensor, model: ResponseModel, target: torch.Tensor) -> torch.Tensor:
+    """Poisson NLL of the arrival-time histogram alone (the calibration objective)."""
+    h, _ = response(theta, model)
+    return poisson_nll(h, target, model.n, model.tally.time_bins)
+
+
+def _to_theta(phi: torch.Tensor) -> torch.Tensor:
+    # phi = (log La, log Ls, log(1 - R), log tau): unconstrained and well scaled
+    e = torch.exp(phi)
+    return torch.stack([e[0], e[1], 1.0 - e[2], e[3]])
+
+
+def calibrate(base: SimParams, theta0, target: np.ndarray, n: int, steps: int = 20,
+              lr: float = 0.04, model: ResponseModel | None = None):
+    """Adam on phi = (log La, log Ls, log(1-R), log tau) minimising the Poisson NLL
+    of the arrival-time histogram; gradients from the adjoint replay. Returns the
+    trajectory [(theta, loss)] including the final point."""
+    own = model is None
+    model = model or ResponseModel(base, n)
+    tgt = torch.as_tensor(target, dtype=torch.float64)
+    t0 = np.asarray(theta0, np.float64)
+    phi = torch.tensor([math.log(t0[0]), math.log(t0[1]), math.log(1.0 - t0[2]), math.log(t0[3])],
+                       dtype=torch.float64, requires_grad=True)
+    opt = torch.optim.Adam([phi], lr=lr)
+    traj = []
+    try:
+        for _ in range(steps):
+            opt.zero_grad()
+            theta = _to_theta(phi)
+            loss = nll_loss(theta, model, tgt)
+            loss.backward()  # adjoint replay, then the chain rule through _to_theta
+            traj.append((theta.detach().numpy().copy(), float(loss.detach())))
+            opt.step()
+        theta = _to_theta(phi).detach().numpy()
+        with torch.no_grad():
+            traj.append((theta.copy(), float(nll_loss(torch.as_tensor(theta), model, tgt))))
+    finally:
+        if own:
+            model.close()
+    return traj

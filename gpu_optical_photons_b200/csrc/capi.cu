@@ -428,6 +428,13 @@ int engine_graph(optx_engine* e, int mode, bool batch, int grid, optx_engine::Gr
   cudaGraphNode_t n_wave;
   OPTX_CUDA(cudaGraphAddKernelNode(&n_wave, body, nullptr, 0, &wp));
   OPTX_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+  // Graphs of one configuration bake its parameters in; keep a few.
+  constexpr size_t kMaxGraphs = 8;
+  if (e->graphs.size() >= kMaxGraphs) {
+    cudaGraphExecDestroy(e->graphs.front().exec);
+    cudaGraphDestroy(e->graphs.front().graph);
+    e->graphs.erase(e->graphs.begin());
+  }
   e->graphs.push_back(g);
   *out = &e->graphs.back();
   return OPTX_OK;
@@ -808,6 +815,35 @@ int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* s
   const DevRecords d = to_dev(dev_out);
   return engine_run(e, kModeRecords, &d, nullptr, 0.0, nullptr, 0u,
                     static_cast<cudaStream_t>(stream));
+}
+
+int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_det,
+                            double* dev_grad, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr || dev_w_bin == nullptr || dev_grad == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "engine, dev_w_bin and dev_grad must not be NULL");
+  if (e->n_events != 1)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "the adjoint runs on a single-configuration batch");
+  const DevParams& P = e->h_params[0];
+  // theta = (abs_length, scat_length, reflectivity, tau) of the uploaded configuration.
+  const double la = P.abs_length, ls = P.scat_length, R = P.refl0, tau = P.tau;
+  uint32_t mask = 0;
+  if (std::isfinite(la)) mask |= 1u;
+  if (std::isfinite(ls)) mask |= 2u;
+  bool painted = false;
+  for (int f = 0; f < 5; ++f) {
+    const uint32_t m = (P.surf_bits >> (2 * f)) & 3u;
+    painted = painted || m == kSpecular || m == kLambertian;
+  }
+  if (painted && R > 0.0) mask |= 4u;
+  if (tau > 0.0) mask |= 8u;
+  const double inv[7] = {1.0 / la, 1.0 / (la * la), 1.0 / ls, 1.0 / (ls * ls),
+                         R > 0.0 ? 1.0 / R : 0.0, tau > 0.0 ? 1.0 / tau : 0.0,
+                         tau > 0.0 ? 1.0 / (tau * tau) : 0.0};
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  OPTX_TRY(engine_run(e, kModeAdjoint, nullptr, dev_w_bin, w_det, inv, mask, st));
+  OPTX_CUDA(cudaMemcpyAsync(dev_grad, e->d_grad, 4 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return OPTX_OK;
 }
 
 int optx_engine_tally_ptr(optx_engine* e, uint64_t** dev_ptr, uint64_t* len_per_event) {

@@ -168,6 +168,20 @@ int optx_engine_run_tally(optx_engine* e, void* stream);
 /* Runs the uploaded batch writing records (device arrays indexed by photon
  * index relative to first_id, total entries = sum of counts). */
 int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* stream);
+/* Path-replay adjoint (extension; the reference has no differentiation).
+ * Replays the uploaded single-configuration batch from the photons' Philox
+ * counters (no stored paths) and accumulates, in FP64, for every detected photon
+ *   grad[j] += (w_bin[time_bin(t)] + w_det) * S_j
+ * with the score S of its history with respect to theta = (abs_length,
+ * scat_length, reflectivity, tau):
+ *   S_La = path / La^2,  S_Ls = path / Ls^2 - n_scatter / Ls,
+ *   S_R = (reflections at painted faces) / R,  S_tau = t_emit / tau^2 - 1 / tau
+ * (terms of a disabled process are 0). With w_bin = dLoss/dh (h = the run's
+ * arrival-time histogram, time_bins + 1 entries) and w_det = dLoss/dD / n
+ * (D = detected fraction), grad = dLoss/dtheta. dev_w_bin, dev_grad (4
+ * doubles, overwritten): device pointers. Asynchronous on `stream`. */
+int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_det,
+                            double* dev_grad, void* stream);
 /* Device pointer of the per-event tallies (n_events x tally length u64). */
 int optx_engine_tally_ptr(optx_engine* e, uint64_t** dev_ptr, uint64_t* len_per_event);
 /* Copies the per-event tallies to host memory (synchronises `stream`). */

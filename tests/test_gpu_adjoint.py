@@ -1,0 +1,128 @@
+"""Path-replay adjoint (optx_engine_run_adjoint behind a torch.autograd.Function):
+against the oracle's FP64 CPU gradient (same estimator, same photons), against
+common-random-number central finite differences (independent estimator of the
+same gradient), its cost relative to one forward run, and a calibration."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from gpu_optical_photons_b200 import params as P
+from gpu_optical_photons_b200.adjoint import (ResponseModel, calibrate, crn_central_fd, loss_fn,
+                                             response, target_histogram, with_theta)
+from gpu_optical_photons_b200.wavefront import WaveConfig
+
+pytestmark = pytest.mark.gpu
+
+BASE = P.config2()[0]                       # wrapped Lambertian, Rayleigh, volume source
+THETA0 = np.array([1000.0, 700.0, 0.95, 4.0])
+THETA_T = np.array([800.0, 600.0, 0.93, 3.5])
+TC = P.TallyConfig(500, 50.0, 1)
+
+
+@pytest.mark.parametrize("math_mode,tol", [("exact", 1e-10), ("fast", 2e-3)])
+def test_adjoint_equals_fp64_oracle_gradient(engine, oracle, math_mode, tol):
+    n = 200_000
+    m = ResponseModel(BASE, n, TC, first_id=5, config=WaveConfig(math=math_mode))
+    try:
+        w = np.random.default_rng(1).normal(size=TC.time_bins + 1)
+        g = m.replay(THETA0, torch.as_tensor(w), 0.7)
+        hist, det = m.forward(THETA0)
+    finally:
+        m.close()
+    mode = oracle.PORTABLE if math_mode == "exact" else oracle.PLATFORM
+    go, ho, do = oracle.adjoint(with_theta(BASE, THETA0), TC, n, w_bin=w, w_det=0.7, first_id=5, mode=mode)
+    assert np.all(np.abs(g - go) <= tol * np.abs(go)), (g, go)
+    if math_mode == "exact":
+        assert np.array_equal(hist, ho.astype(np.float64)) and det == do
+
+
+def _batch_gradients(n_batch, k_batches, fn_adj, fn_fd):
+    G, F = [], []
+    for k in range(k_batches):
+        m = ResponseModel(BASE, n_batch, TC, first_id=k * n_batch)
+        try:
+            G.append(fn_adj(m))
+            F.append(fn_fd(m))
+        finally:
+            m.close()
+    G, F = np.array(G), np.array(F)
+    D = G - F
+    z = D.mean(0) / (D.std(0, ddof=1) / math.sqrt(k_batches))
+    return G.mean(0), F.mean(0), z
+
+
+def test_loss_gradient_within_2_sigma_of_crn_fd(engine):
+    """Loss = Poisson NLL of the 500-bin histogram (target: theta_T, seed 777) + D."""
+    nb, kb = 1_000_000, 16
+    target = target_histogram(BASE, THETA_T, nb, seed=777, tally=TC)
+    tgt = torch.as_tensor(target)
+
+    def adj(m):
+        th = torch.tensor(THETA0, requires_grad=True)
+        loss_fn(th, m, tgt).backward()
+        return th.grad.numpy().copy()
+
+    g, f, z = _batch_gradients(nb, kb, adj, lambda m: crn_central_fd(THETA0, m, target, 1e-3))
+    print("adjoint", g, "crn fd", f, "z", z)
+    assert np.all(np.abs(z) < 2.0), z
+    assert np.all(np.sign(g) == np.sign(f))
+
+
+def test_detected_fraction_gradient_within_2_sigma_of_crn_fd(engine):
+    nb, kb = 1_000_000, 16
+
+    def adj(m):
+        th = torch.tensor(THETA0, requires_grad=True)
+        _, d = response(th, m)
+        d.backward()
+        return th.grad.numpy().copy()
+
+    def fd(m):
+        out = np.zeros(4)
+        for j in range(4):
+            up, dn = THETA0.copy(), THETA0.copy()
+            up[j] = float(np.float32(THETA0[j] * 1.001))
+            dn[j] = float(np.float32(THETA0[j] * 0.999))
+            out[j] = (m.forward(up)[1] - m.forward(dn)[1]) / m.n / (up[j] - dn[j])
+        return out
+
+    g, f, z = _batch_gradients(nb, kb, adj, fd)
+    print("dD/dtheta adjoint", g, "crn fd", f, "z", z)
+    # tau does not change detection: both estimates are noise around 0
+    assert np.all(np.abs(z) < 2.0), z
+
+
+def test_adjoint_cost_at_most_1p5_forward(engine):
+    n = 10_000_000
+    m = ResponseModel(BASE, n, TC)
+    try:
+        w = torch.ones(TC.time_bins + 1, dtype=torch.float64)
+        th = THETA0
+        m.forward(th)
+        m.replay(th, w, 0.5)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fwd, adj = [], []
+        for _ in range(3):
+            s.record(); m.engine.run_tally(); e.record(); torch.cuda.synchronize()
+            fwd.append(s.elapsed_time(e))
+            s.record(); m.replay(th, w, 0.5); e.record(); torch.cuda.synchronize()
+            adj.append(s.elapsed_time(e))
+    finally:
+        m.close()
+    ratio = min(adj) / min(fwd)
+    print(f"forward {min(fwd):.3f} ms, adjoint replay {min(adj):.3f} ms, ratio {ratio:.3f}")
+    assert ratio <= 1.5
+
+
+def test_calibration_reduces_loss_and_recovers_tau(engine):
+    n = 4_000_000
+    target = target_histogram(BASE, THETA_T, n, seed=777, tally=TC)
+    traj = calibrate(BASE, THETA0, target, n, steps=20)
+    l0, l1 = traj[0][1], traj[-1][1]
+    th = traj[-1][0]
+    print("calibration", [(np.round(t, 4).tolist(), round(l, 6)) for t, l in traj])
+    assert l1 < l0
+    # the arrival-time shape pins tau; the loss-rate parameters are partly degenerate
+    assert abs(th[3] - THETA_T[3]) < abs(THETA0[3] - THETA_T[3]) / 2
