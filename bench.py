@@ -15,8 +15,11 @@ batch: one CUDA-graph launch of the persistent wavefront engine.
 ``--impl reference`` times the reference's own CPU implementation
 (run_cpu_tally of the reference backend, compiled from its sources into
 oracle/_ref; the oracle port when that is absent) on the same workload.
-Multi-GPU (torchrun): every rank runs its own copy of the batch (independent
-events, no collective on the data path), value = all ranks' steps / max time.
+Multi-GPU (torchrun): every rank transports its own shard of photons (the same
+event list with photon ids offset by rank x photons, so shards are disjoint;
+no collective on the data path), value = all ranks' steps / max time over ranks.
+The engine settings (register budget, compaction threshold, block size,
+cadence, queue depth) come from the autotuner unless given on the command line.
 """
 from __future__ import annotations
 
@@ -56,6 +59,7 @@ def parse():
     ap.add_argument("--threshold", type=int, default=0, help="0: tuned default")
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--bps", type=int, default=0, help="resident blocks per SM (register budget)")
+    ap.add_argument("--no-autotune", action="store_true", help="use the default engine settings")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--events", type=int, default=4096)
     ap.add_argument("--host-loop", action="store_true",
@@ -203,12 +207,20 @@ def run_optx(args):
     from gpu_optical_photons_b200 import _lib
     from gpu_optical_photons_b200.params import CSimParams, TallyConfig
     from gpu_optical_photons_b200.wavefront import WaveConfig, WavefrontEngine, batched_events
+    from gpu_optical_photons_b200.distributed import max_over_ranks, shard_first_id
 
     events, counts = batched_events(n_events=args.events)
     n_photons = int(counts.sum())
+    first_id = shard_first_id(rank, n_photons)  # disjoint photon ids per rank
     tc = TallyConfig(100, 50.0, 10)
     cfg = WaveConfig(block_size=args.block or 256, threshold=args.threshold or 28,
-                     blocks_per_sm=args.bps, use_graph=not args.host_loop)
+                     blocks_per_sm=args.bps or 3, use_graph=not args.host_loop)
+    tuned = None
+    if not args.no_autotune and not args.host_loop and not (args.threshold or args.bps or args.block):
+        from gpu_optical_photons_b200.autotune import tune
+        t0 = time.perf_counter()
+        cfg, tune_log = tune(events, counts, tc, base=cfg, repeats=2)
+        tuned = {"seconds": round(time.perf_counter() - t0, 1), "candidates": len(tune_log)}
     eng = WavefrontEngine(tc, len(events), n_photons, cfg)
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
@@ -222,7 +234,7 @@ def run_optx(args):
     h2d_bytes = len(events) * 112 + (len(events) + 1) * 8 + 256   # DevParams table + offsets + run args
     d2h_bytes = len(events) * tc.length * 8 + 64                  # tallies + control block
 
-    eng.set_events(events, counts, 0, stream=sptr)
+    eng.set_events(events, counts, first_id, stream=sptr)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
     # warm-up
@@ -255,9 +267,7 @@ def run_optx(args):
     st = eng.stats(stream=sptr)
     waves = int(st["launches"])
     if pg:
-        t = torch.tensor([ms_step], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_step = float(t.item())
+        ms_step = max_over_ranks(ms_step, pg, device="cuda")
     value = world * steps_per_run / (ms_step * 1e-3)
 
     # e2e: the C ABI call with host buffers (H2D table, run, D2H tallies) per step.
@@ -270,7 +280,7 @@ def run_optx(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         _lib.check(L.optx_run_batch(eng._h, ctypes.c_void_p(ev_pinned.data_ptr()), None,
-                                    ctypes.c_void_p(cnt_pinned.data_ptr()), len(events), 0,
+                                    ctypes.c_void_p(cnt_pinned.data_ptr()), len(events), first_id,
                                     ctypes.c_void_p(out_pinned.data_ptr()), ctypes.byref(sts),
                                     ctypes.byref(tmg)))
         dt = (time.perf_counter() - t0) * 1e3
@@ -278,9 +288,7 @@ def run_optx(args):
             e2e_ms.append(dt)
     e2e_step = float(np.mean(e2e_ms))
     if pg:
-        t = torch.tensor([e2e_step], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_step = float(t.item())
+        e2e_step = max_over_ranks(e2e_step, pg, device="cuda")
     assert np.array_equal(out_pinned.numpy().astype(np.uint64), tallies)
 
     clocks = clk.summary()
@@ -311,7 +319,9 @@ def run_optx(args):
                    "events": len(events), "photons_per_step": n_photons,
                    "photon_steps_per_step": steps_per_run, "photons_per_s": world * n_photons / (ms_step * 1e-3),
                    "l2": "flushed between timed steps (256 MB write, outside the CUDA events)",
+                   "autotune": tuned,
                    "engine": {"block_size": cfg.block_size, "threshold": cfg.threshold,
+                              "wave_quota": cfg.wave_quota,
                               "blocks_per_sm": cfg.blocks_per_sm,
                               "cadence": cfg.cadence, "graph": cfg.use_graph, "math": cfg.math},
                    "parallelism": f"dp{world} (independent event batches per GPU)"},

@@ -1,0 +1,125 @@
+"""Autotuner of the wavefront engine.
+
+Chooses, for a given workload (a batch of events with their photon counts and
+a tally configuration), the engine settings by measurement on the device:
+
+* ``blocks_per_sm`` — resident 256-thread blocks per SM, i.e. the register
+  budget of the wave kernel (2, 3 or 4 blocks: <= 128 / 80 / 64 registers);
+* ``threshold`` — refill a warp when fewer than this many lanes are alive (the
+  compaction threshold: higher keeps warps fuller, lower refills less often);
+* ``block_size`` — threads per block;
+* ``cadence`` — forced compaction after this many steps in a wave (0 = only when
+  the wave's work runs out);
+* ``wave_quota`` — fresh photons admitted per wave, i.e. the depth of the work
+  queue between two compactions (0 = all photons in the first wave).
+
+Staged coordinate search: (blocks_per_sm x threshold) first, then block size,
+cadence and queue depth around the best point. Each candidate is timed with
+CUDA events on the launching stream (median of `repeats` runs after one warm-up
+run), on the real workload. Every candidate computes the same tallies (the
+engine's results do not depend on these settings), which `tune` checks.
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import time
+from dataclasses import asdict, replace
+
+import numpy as np
+
+from .params import TallyConfig
+from .wavefront import WaveConfig, WavefrontEngine
+
+
+def time_config(cfg: WaveConfig, events, counts, tally: TallyConfig, repeats: int = 3,
+                first_id: int = 0):
+    """(median ms per run, tallies, stats) of one engine configuration."""
+    import torch
+    eng = WavefrontEngine(tally, len(events), int(np.sum(counts)), cfg)
+    try:
+        eng.set_events(events, counts, first_id)
+        eng.run_tally()  # warm-up: graph instantiation, caches
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = []
+        for _ in range(repeats):
+            s.record()
+            eng.run_tally()
+            e.record()
+            torch.cuda.synchronize()
+            ms.append(s.elapsed_time(e))
+        return float(np.median(ms)), eng.tallies(), eng.stats()
+    finally:
+        eng.close()
+
+
+def tune(events, counts, tally: TallyConfig, base: WaveConfig | None = None, repeats: int = 3,
+         bps=(2, 3, 4), thresholds=(16, 20, 24, 28, 32), blocks=(128, 256), cadences=(0, 32),
+         quota_fracs=(0.0, 0.25), verbose: bool = False):
+    """Returns (best WaveConfig, list of measurement dicts)."""
+    base = base or WaveConfig()
+    total = int(np.sum(counts))
+    log = []
+    ref_tallies = None
+
+    def measure(cfg):
+        nonlocal ref_tallies
+        t0 = time.perf_counter()
+        ms, tallies, st = time_config(cfg, events, counts, tally, repeats)
+        if ref_tallies is None:
+            ref_tallies = tallies
+        elif not np.array_equal(tallies, ref_tallies):
+            raise AssertionError(f"engine settings changed the tallies: {cfg}")
+        rec = {**asdict(cfg), "ms": ms, "simt": st["simt_efficiency"], "waves": st["launches"],
+               "tune_s": time.perf_counter() - t0}
+        log.append(rec)
+        if verbose:
+            print(json.dumps(rec), flush=True)
+        return ms
+
+    best_cfg, best_ms = None, float("inf")
+    for b, t in itertools.product(bps, thresholds):
+        cfg = replace(base, blocks_per_sm=b, threshold=t)
+        ms = measure(cfg)
+        if ms < best_ms:
+            best_cfg, best_ms = cfg, ms
+    for bs in blocks:
+        if bs == best_cfg.block_size:
+            continue
+        cfg = replace(best_cfg, block_size=bs)  # same register budget, smaller blocks
+        ms = measure(cfg)
+        if ms < best_ms:
+            best_cfg, best_ms = cfg, ms
+    for c in cadences:
+        if c == best_cfg.cadence:
+            continue
+        cfg = replace(best_cfg, cadence=c)
+        ms = measure(cfg)
+        if ms < best_ms:
+            best_cfg, best_ms = cfg, ms
+    for f in quota_fracs:
+        q = int(total * f)
+        if q == best_cfg.wave_quota:
+            continue
+        cfg = replace(best_cfg, wave_quota=q)
+        ms = measure(cfg)
+        if ms < best_ms:
+            best_cfg, best_ms = cfg, ms
+    return best_cfg, log
+
+
+def main(argv=None):
+    import argparse
+    from .wavefront import batched_events
+    ap = argparse.ArgumentParser(description="tune the wavefront engine on the batched workload")
+    ap.add_argument("--events", type=int, default=4096)
+    ap.add_argument("--repeats", type=int, default=3)
+    a = ap.parse_args(argv)
+    events, counts = batched_events(n_events=a.events)
+    best, log = tune(events, counts, TallyConfig(100, 50.0, 10), repeats=a.repeats, verbose=True)
+    print(json.dumps({"best": asdict(best), "ms": min(r["ms"] for r in log)}))
+
+
+if __name__ == "__main__":
+    main()

@@ -63,10 +63,10 @@ __device__ __forceinline__ uint32_t transport(const DevParams& P, uint64_t id, P
                                               ScoreAux& aux) {
   Rng r;
   r.init(id, P.key_lo, P.key_hi, 0u);
-  start_photon<AUX>(P, s, r, aux);
+  start_photon<AUX>(P, s, r, id, aux);
   uint32_t fate = kMaxSteps;
   for (uint32_t step = 0; step < P.max_steps; ++step) {
-    if (!step_photon<AUX>(P, s, r, fate, aux)) break;
+    if (!step_photon<AUX>(P, s, r, id, fate, aux)) break;
   }
   return fate;
 }
@@ -228,18 +228,39 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
   double* s_w = reinterpret_cast<double*>(extra);
   __shared__ double s_red[4][16];
 
-  const uint32_t wave = ctrl->wave;
-  const uint32_t n_in = ctrl->n_in;
-  const uint32_t items = n_in + ctrl->fresh_count;
-  const unsigned long long fresh_next = ctrl->fresh_next;
-  const float4* __restrict__ qin = (wave & 1u) ? A->qb : A->qa;
-  float4* __restrict__ qout = (wave & 1u) ? A->qa : A->qb;
-  const uint32_t T = A->threshold;
-  const uint32_t cadence = A->cadence;
-  const uint32_t qcap = A->qcap;
-  const unsigned long long first_id = A->first_id;
-  const unsigned long long iter_cap = A->iter_cap;
-  const TallyDev tc = A->tc;
+  // Wave-constant values live in shared memory, not in each thread's registers.
+  struct WaveShared {
+    const float4* qin;
+    float4* qout;
+    unsigned long long fresh_next, first_id, iter_cap;
+    uint32_t n_in, items, T, cadence, qcap;
+    TallyDev tc;
+  };
+  __shared__ WaveShared ws;
+  if (threadIdx.x == 0) {
+    const uint32_t wave = ctrl->wave;
+    ws.n_in = ctrl->n_in;
+    ws.items = ws.n_in + ctrl->fresh_count;
+    ws.fresh_next = ctrl->fresh_next;
+    ws.qin = (wave & 1u) ? A->qb : A->qa;
+    ws.qout = (wave & 1u) ? A->qa : A->qb;
+    ws.T = A->threshold;
+    ws.cadence = A->cadence;
+    ws.qcap = A->qcap;
+    ws.first_id = A->first_id;
+    ws.iter_cap = A->iter_cap;
+    ws.tc = A->tc;
+  }
+  __syncthreads();
+  const uint32_t& n_in = ws.n_in;
+  const uint32_t& items = ws.items;
+  const unsigned long long& fresh_next = ws.fresh_next;
+  const uint32_t& T = ws.T;
+  const uint32_t& cadence = ws.cadence;
+  const uint32_t& qcap = ws.qcap;
+  const unsigned long long& first_id = ws.first_id;
+  const unsigned long long& iter_cap = ws.iter_cap;
+  const TallyDev& tc = ws.tc;
 
   if (MODE == kModeTally && !BATCH) {
     for (uint32_t b = threadIdx.x; b < tc.len - 7u; b += blockDim.x) s_hist[b] = 0u;
@@ -345,7 +366,7 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
     if (spill) {
       const uint32_t slot = base + static_cast<uint32_t>(__popc(smask & lt));
       if (slot < qcap) {
-        float4* q = qout + qidx(slot);
+        float4* q = ws.qout + qidx(slot);
         q[0] = make_float4(s.px, s.py, s.pz, s.t);
         q[32] = make_float4(s.dx, s.dy, s.dz, s.path);
         q[64] = make_float4(__uint_as_float(s.nb), __uint_as_float(s.ns),
@@ -384,15 +405,17 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
           uint32_t npidx, nev = 0u;
           if (item < n_in) {
             // A survivor of the previous wave: 4 x 128-bit loads from its tile.
-            const float4* q = qin + qidx(item);
+            const float4* q = ws.qin + qidx(item);
             const float4 a = q[0], b = q[32], c = q[64], d = q[96];
             ns.px = a.x; ns.py = a.y; ns.pz = a.z; ns.t = a.w;
             ns.dx = b.x; ns.dy = b.y; ns.dz = b.z; ns.path = b.w;
             ns.nb = __float_as_uint(c.x);
             ns.ns = __float_as_uint(c.y);
             npidx = __float_as_uint(c.w);
-            na_aux.n_refl = __float_as_uint(d.x);
-            na_aux.t_emit = d.y;
+            if (MODE == kModeAdjoint) {
+              na_aux.n_refl = __float_as_uint(d.x);
+              na_aux.t_emit = d.y;
+            }
             nev = __float_as_uint(d.z);
             const DevParams& P = params_of<BATCH>(P0, A, nev);
             nr.init(first_id + npidx, P.key_lo, P.key_hi, __float_as_uint(c.z));
@@ -402,7 +425,7 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
             if (BATCH) nev = find_event(A, g);
             const DevParams& P = params_of<BATCH>(P0, A, nev);
             nr.init(first_id + g, P.key_lo, P.key_hi, 0u);
-            start_photon<MODE == kModeAdjoint>(P, ns, nr, na_aux);
+            start_photon<MODE == kModeAdjoint>(P, ns, nr, first_id + g, na_aux);
           }
           float4* e = pantry + (pc + lane) * 7u;
           e[0] = make_float4(ns.px, ns.py, ns.pz, ns.t);
@@ -410,8 +433,13 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
           e[2] = make_uint4_as_float4(ns.nb, ns.ns, npidx, nev);
           e[3] = make_uint4_as_float4(nr.w[0], nr.w[1], nr.w[2], nr.w[3]);
           e[4] = make_uint4_as_float4(nr.w[4], nr.w[5], nr.w[6], nr.w[7]);
-          e[5] = make_float4(__uint_as_float(nr.o), __uint_as_float(nr.blk),
-                             __uint_as_float(na_aux.n_refl), na_aux.t_emit);
+          if (MODE == kModeAdjoint) {
+            e[5] = make_float4(__uint_as_float(nr.o), __uint_as_float(nr.blk),
+                               __uint_as_float(na_aux.n_refl), na_aux.t_emit);
+          } else {
+            reinterpret_cast<float2*>(e + 5)[0] =
+                make_float2(__uint_as_float(nr.o), __uint_as_float(nr.blk));
+          }
         }
         pc += got;
         __syncwarp();
@@ -422,7 +450,7 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
         const uint32_t rank = static_cast<uint32_t>(__popc(~amask & lt));
         if (!alive && rank < take) {
           const float4* e = pantry + (pc - 1u - rank) * 7u;
-          const float4 a = e[0], b = e[1], c = e[2], d = e[3], f = e[4], h = e[5];
+          const float4 a = e[0], b = e[1], c = e[2], d = e[3], f = e[4];
           s.px = a.x; s.py = a.y; s.pz = a.z; s.t = a.w;
           s.dx = b.x; s.dy = b.y; s.dz = b.z; s.path = b.w;
           s.nb = __float_as_uint(c.x);
@@ -433,16 +461,18 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
           r.w[2] = __float_as_uint(d.z); r.w[3] = __float_as_uint(d.w);
           r.w[4] = __float_as_uint(f.x); r.w[5] = __float_as_uint(f.y);
           r.w[6] = __float_as_uint(f.z); r.w[7] = __float_as_uint(f.w);
-          r.o = __float_as_uint(h.x);
-          r.blk = __float_as_uint(h.y);
-          aux.n_refl = __float_as_uint(h.z);
-          aux.t_emit = h.w;
+          if (MODE == kModeAdjoint) {
+            const float4 h = e[5];
+            r.o = __float_as_uint(h.x);
+            r.blk = __float_as_uint(h.y);
+            aux.n_refl = __float_as_uint(h.z);
+            aux.t_emit = h.w;
+          } else {
+            const float2 h = reinterpret_cast<const float2*>(e + 5)[0];
+            r.o = __float_as_uint(h.x);
+            r.blk = __float_as_uint(h.y);
+          }
           const DevParams& P = params_of<BATCH>(P0, A, ev);
-          const unsigned long long id = first_id + pidx;
-          r.id_lo = static_cast<uint32_t>(id);
-          r.id_hi = static_cast<uint32_t>(id >> 32);
-          r.k0 = P.key_lo;
-          r.k1 = P.key_hi;
           wsteps = 0u;
           alive = s.nb + s.ns < P.max_steps;
           if (!alive) finish(kMaxSteps, P);
@@ -468,7 +498,7 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
     if (alive) {
       const DevParams& P = params_of<BATCH>(P0, A, ev);
       uint32_t fate = kMaxSteps;
-      const bool still = step_photon<MODE == kModeAdjoint>(P, s, r, fate, aux);
+      const bool still = step_photon<MODE == kModeAdjoint>(P, s, r, first_id + pidx, fate, aux);
       ++wsteps;
       if (!still) {
         alive = false;

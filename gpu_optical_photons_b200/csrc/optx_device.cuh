@@ -95,27 +95,26 @@ __device__ __forceinline__ float to_uniform(uint32_t bits) {
 // Invariant between steps: w[0..3] = block `blk`, w[4..7] = block `blk + 1`,
 // next unread word at w[o], o in [0, 3]; so a step can read 5 words.
 // draws() = 4 * blk + o is the reference's PhiloxStream::draws().
+// The photon id and key are not stored: callers pass them (the key lives in the
+// parameters, the id is first id + photon index), which keeps the per-lane state
+// at 10 registers.
 struct Rng {
   uint32_t w[8];
   uint32_t o, blk;
-  uint32_t id_lo, id_hi, k0, k1;
 
-  __device__ __forceinline__ void fill(uint32_t block) {
-    const uint4 a = philox10(make_uint4(block, 0u, id_lo, id_hi), k0, k1);
-    const uint4 b = philox10(make_uint4(block + 1u, 0u, id_lo, id_hi), k0, k1);
-    w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
-    w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
-    blk = block;
-  }
   // Starts (draws = 0) or resumes the stream of photon `id` after `draws` words
-  // (philox.hpp:117-134).
+  // (philox.hpp:117-134): blocks draws/4 and draws/4 + 1 fill the window.
   __device__ __forceinline__ void init(uint64_t id, uint32_t key_lo, uint32_t key_hi,
                                        uint32_t draws) {
-    id_lo = static_cast<uint32_t>(id);
-    id_hi = static_cast<uint32_t>(id >> 32);
-    k0 = key_lo;
-    k1 = key_hi;
-    fill(draws >> 2);
+    const uint32_t block = draws >> 2;
+#pragma unroll 1
+    for (uint32_t j = 0; j < 2u; ++j) {
+      const uint4 b = philox10(make_uint4(block + j, 0u, static_cast<uint32_t>(id),
+                                          static_cast<uint32_t>(id >> 32)), key_lo, key_hi);
+      w[0] = w[4]; w[1] = w[5]; w[2] = w[6]; w[3] = w[7];
+      w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
+    }
+    blk = block;
     o = draws & 3u;
   }
   __device__ __forceinline__ uint32_t draws() const { return 4u * blk + o; }
@@ -131,13 +130,15 @@ struct Rng {
   __device__ __forceinline__ float uniform() const { return to_uniform(word<I>()); }
 
   // Consumes k words; slides the window (one Philox call per block used up).
-  __device__ __forceinline__ void advance(uint32_t k) {
+  __device__ __forceinline__ void advance(uint32_t k, uint64_t id, uint32_t key_lo,
+                                          uint32_t key_hi) {
     o += k;
 #pragma unroll 1
     while (o >= 4u) {
       w[0] = w[4]; w[1] = w[5]; w[2] = w[6]; w[3] = w[7];
       ++blk;
-      const uint4 b = philox10(make_uint4(blk + 1u, 0u, id_lo, id_hi), k0, k1);
+      const uint4 b = philox10(make_uint4(blk + 1u, 0u, static_cast<uint32_t>(id),
+                                          static_cast<uint32_t>(id >> 32)), key_lo, key_hi);
       w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
       o -= 4u;
     }
@@ -248,7 +249,10 @@ __device__ __forceinline__ void rotate_about(float ax, float ay, float az, float
 __device__ __forceinline__ float rayleigh_cos(float u) {
   const float q = 4.0f * u - 2.0f;
   const float s = sqrtf(q * q + 1.0f);
-  const float a = (q >= 0.0f) ? m_cbrt(q + s) : 1.0f / m_cbrt(s - q);
+  // One cube-root call site: cbrt(q + s) for q >= 0, 1 / cbrt(s - q) otherwise.
+  const bool pos = q >= 0.0f;
+  const float c = m_cbrt(pos ? q + s : s - q);
+  const float a = pos ? c : 1.0f / c;
   return fminf(1.0f, fmaxf(-1.0f, a - 1.0f / a));
 }
 
@@ -267,7 +271,8 @@ __device__ __forceinline__ float fresnel_R(float n1, float n2, float eta2, float
 // Emission (transport.hpp:55-67): position (3 draws, volume source only),
 // isotropic direction (2), exponential emission time (1).
 template <bool AUX>
-__device__ __forceinline__ void start_photon(const DevParams& P, Photon& s, Rng& r, ScoreAux& aux) {
+__device__ __forceinline__ void start_photon(const DevParams& P, Photon& s, Rng& r, uint64_t id,
+                                             ScoreAux& aux) {
   uint32_t k;
   if (P.source == 0u) {
     s.px = P.src_x;
@@ -295,15 +300,15 @@ __device__ __forceinline__ void start_photon(const DevParams& P, Photon& s, Rng&
   s.path = 0.0f;
   s.nb = 0u;
   s.ns = 0u;
-  r.advance(k);
+  r.advance(k, id, P.key_lo, P.key_hi);
 }
 
 // One step (transport.hpp:71-145). Returns true while the photon is alive;
 // otherwise `fate` is set and the photon sits at its final interaction.
 // The window is advanced only for photons that stay alive.
 template <bool AUX>
-__device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& r, uint32_t& fate,
-                                            ScoreAux& aux) {
+__device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& r, uint64_t id,
+                                            uint32_t& fate, ScoreAux& aux) {
   const float u_abs = r.uniform<0>(), u_sca = r.uniform<1>();
   const float s_abs = (P.abs_length == kInf) ? kInf : -P.abs_length * m_log(u_abs);
   const float s_sca = (P.scat_length == kInf) ? kInf : -P.scat_length * m_log(u_sca);
@@ -412,7 +417,7 @@ __device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& 
     if (axis == 1) s.dy = -s.dy;
     if (axis == 2) s.dz = -s.dz;
   }
-  r.advance(k);
+  r.advance(k, id, P.key_lo, P.key_hi);
   return true;
 }
 
