@@ -156,14 +156,19 @@ __device__ __forceinline__ uint32_t find_event(const WaveArgs* __restrict__ A, u
   return e;
 }
 
-// table[k] = the event that holds photon k << kEvShift (one thread per event).
+// table[k] = the event that holds photon k << kEvShift: the largest e with
+// offsets[e] <= k << kEvShift, which is never an empty event (one thread per entry).
 __global__ void event_table_kernel(const unsigned long long* __restrict__ offsets, uint32_t n_events,
                                    uint32_t* __restrict__ table, unsigned long long total) {
-  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n_events) return;
-  const unsigned long long lo = offsets[e], hi = offsets[e + 1] < total ? offsets[e + 1] : total;
-  for (unsigned long long k = (lo + (1ull << kEvShift) - 1ull) >> kEvShift; (k << kEvShift) < hi; ++k)
-    table[k] = e;
+  const unsigned long long k = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned long long g = k << kEvShift;
+  if (g >= total) return;
+  uint32_t lo = 0, hi = n_events;
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (offsets[mid] <= g) lo = mid; else hi = mid;
+  }
+  table[k] = lo;
 }
 
 __device__ __forceinline__ float4 make_uint4_as_float4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
@@ -677,7 +682,9 @@ cudaError_t launch_wave(int mode, bool batch, int minb, const DevParams& P, cons
 
 cudaError_t launch_event_table(const unsigned long long* offsets, uint32_t n_events,
                                uint32_t* table, unsigned long long total, cudaStream_t st) {
-  event_table_kernel<<<(n_events + 255) / 256, 256, 0, st>>>(offsets, n_events, table, total);
+  const unsigned long long entries = ((total + (1ull << kEvShift) - 1ull) >> kEvShift);
+  event_table_kernel<<<static_cast<unsigned>((entries + 255) / 256), 256, 0, st>>>(offsets, n_events,
+                                                                                 table, total);
   return cudaGetLastError();
 }
 
