@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--bps", type=int, default=0, help="resident blocks per SM (register budget)")
     ap.add_argument("--no-autotune", action="store_true", help="use the default engine settings")
+    ap.add_argument("--math", default="fast", choices=["fast", "exact", "approx"],
+                    help="math mode of the kernels (see include/optx.h)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--events", type=int, default=4096)
     ap.add_argument("--host-loop", action="store_true",
@@ -214,7 +216,7 @@ def run_optx(args):
     first_id = shard_first_id(rank, n_photons)  # disjoint photon ids per rank
     tc = TallyConfig(100, 50.0, 10)
     cfg = WaveConfig(block_size=args.block or 256, threshold=args.threshold or 28,
-                     blocks_per_sm=args.bps or 3, use_graph=not args.host_loop)
+                     blocks_per_sm=args.bps or 3, use_graph=not args.host_loop, math=args.math)
     tuned = None
     if not args.no_autotune and not args.host_loop and not (args.threshold or args.bps or args.block):
         from gpu_optical_photons_b200.autotune import tune

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "liboptx.so")
 OK = 0
 ERR_NAMES = {1: "invalid argument", 2: "runtime error", 3: "CUDA error", 4: "no device",
              5: "queue capacity", 6: "watchdog"}
-MATH = {"fast": 0, "exact": 1}
+MATH = {"fast": 0, "exact": 1, "approx": 2}
 
 
 class OptxError(RuntimeError):

@@ -1,8 +1,8 @@
 """Builds liboptx.so in-tree with nvcc for sm_100a.
 
-kernels.cu is compiled twice: once with CUDA's math library and FMA
-contraction (namespace optx::fast) and once with the portable math and
--fmad=false (namespace optx::exact). The CUDA runtime is linked statically so
+kernels.cu is compiled three times: with CUDA's math library and FMA
+contraction (namespace optx::fast), with the portable math and -fmad=false
+(namespace optx::exact), and with --use_fast_math (namespace optx::approx). The CUDA runtime is linked statically so
 the library does not depend on the runtime version another module (torch) has
 loaded. Run ``python -m gpu_optical_photons_b200.build`` or call ``build()``.
 """
@@ -11,6 +11,7 @@ from __future__ import annotations
 import os
 import shutil
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -54,17 +55,22 @@ def build(force: bool = False, verbose: bool = False) -> str:
     units = [
         ("kernels_fast.o", "kernels.cu", ["-DOPTX_NS=fast", "-DOPTX_EXACT=0"]),
         ("kernels_exact.o", "kernels.cu", ["-DOPTX_NS=exact", "-DOPTX_EXACT=1", "-fmad=false"]),
+        ("kernels_approx.o", "kernels.cu", ["-DOPTX_NS=approx", "-DOPTX_EXACT=0", "--use_fast_math"]),
         ("capi.o", "capi.cu", []),
     ]
-    objs = []
+    cmds, objs = [], []
     for obj, src, extra in units:
         out = os.path.join(BUILD, obj)
         cmd = [cc] + ARCH + COMMON + extra + ["-c", os.path.join(CSRC, src), "-o", out]
         if verbose:
             cmd += ["-Xptxas", "-v"]
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(out)
+    with ThreadPoolExecutor(max_workers=len(cmds)) as pool:  # independent units
+        for r in pool.map(lambda c: subprocess.run(c, check=False), cmds):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = LIB + ".tmp"
     cmd = [cc] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lpthread", "-ldl", "-lrt"]
     subprocess.run(cmd, check=True)

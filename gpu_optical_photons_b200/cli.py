@@ -29,7 +29,7 @@ def main(argv=None):
     ap.add_argument("--engine", default="history", choices=["history", "wave"])
     ap.add_argument("--mode", default="tally", choices=["tally", "records"])
     ap.add_argument("--n", type=float, default=1e6)
-    ap.add_argument("--math", default="fast", choices=["fast", "exact"])
+    ap.add_argument("--math", default="fast", choices=["fast", "exact", "approx"])
     ap.add_argument("--block", type=int, default=256)
     ap.add_argument("--threshold", type=int, default=24)
     ap.add_argument("--cadence", type=int, default=0)

@@ -141,8 +141,9 @@ int check_block(int block) {
 }
 
 int check_math(int math) {
-  if (math != OPTX_MATH_FAST && math != OPTX_MATH_EXACT)
-    return fail(OPTX_ERR_INVALID_ARGUMENT, "math must be OPTX_MATH_FAST or OPTX_MATH_EXACT");
+  if (math != OPTX_MATH_FAST && math != OPTX_MATH_EXACT && math != OPTX_MATH_APPROX)
+    return fail(OPTX_ERR_INVALID_ARGUMENT,
+                "math must be OPTX_MATH_FAST, OPTX_MATH_EXACT or OPTX_MATH_APPROX");
   return OPTX_OK;
 }
 
@@ -164,7 +165,10 @@ int num_sms() {
 }
 
 // ---- math-mode dispatch -------------------------------------------------------
-#define DISPATCH(math, fn, ...) ((math) == OPTX_MATH_EXACT ? exact::fn(__VA_ARGS__) : fast::fn(__VA_ARGS__))
+#define DISPATCH(math, fn, ...)                          \
+  ((math) == OPTX_MATH_EXACT    ? exact::fn(__VA_ARGS__)  \
+   : (math) == OPTX_MATH_APPROX ? approx::fn(__VA_ARGS__) \
+                                : fast::fn(__VA_ARGS__))
 
 // ---- cached device buffers (per process; the library serialises calls) ---------
 struct Cache {

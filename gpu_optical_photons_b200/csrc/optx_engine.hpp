@@ -97,5 +97,6 @@ constexpr unsigned kErrQueue = 1u, kErrWatchdog = 2u;
 
 OPTX_DECLARE_LAUNCHERS(fast)
 OPTX_DECLARE_LAUNCHERS(exact)
+OPTX_DECLARE_LAUNCHERS(approx)
 
 }  // namespace optx

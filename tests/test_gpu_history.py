@@ -28,11 +28,12 @@ def test_exact_mode_bitwise_equals_reference_portable_build(engine, golden, name
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)
-def test_fast_mode_agrees_with_reference_default_build(engine, golden, name):
+@pytest.mark.parametrize("math_mode", ["fast", "approx"])
+def test_fast_mode_agrees_with_reference_default_build(engine, golden, name, math_mode):
     arrays, meta = golden
     case = meta["cases"][name]
     p = params_from_meta(case["params"])
-    rec, _ = engine.run_gpu_records(p, case["n"], first_id=case["first_id"], math="fast")
+    rec, _ = engine.run_gpu_records(p, case["n"], first_id=case["first_id"], math=math_mode)
     h = compare_histories(rec, golden_records(arrays, name, "platform"))
     # Tolerance: at most 0.1% of histories with a different discrete path (north star).
     assert h["same_discrete"] >= 0.999 * case["n"] - 1, h
@@ -62,11 +63,12 @@ def test_exact_mode_bitwise_equals_oracle(engine, oracle, name):
 
 
 @pytest.mark.parametrize("name", list(PARITY))
-def test_fast_mode_fate_agreement(engine, oracle, name):
+@pytest.mark.parametrize("math_mode", ["fast", "approx"])
+def test_fast_mode_fate_agreement(engine, oracle, name, math_mode):
     """>= 99.9% of photons with the same fate and step counts as the CPU FP32 run."""
     p = PARITY[name]
     n = 1_000_000
-    rec, _ = engine.run_gpu_records(p, n, math="fast")
+    rec, _ = engine.run_gpu_records(p, n, math=math_mode)
     ref = oracle.records(p, n, 0, mode=oracle.PLATFORM)
     h = compare_histories(rec, ref)
     assert h["fate_differs"] <= 0.001 * n, h

@@ -33,7 +33,7 @@ def test_event_records_identical_to_history(engine, setup, k):
     WaveConfig(threshold=1), WaveConfig(threshold=32), WaveConfig(threshold=16, cadence=4),
     WaveConfig(threshold=24, wave_quota=50_000), WaveConfig(block_size=128, threshold=8),
     WaveConfig(use_graph=False, threshold=20, cadence=7, wave_quota=30_000)])
-@pytest.mark.parametrize("math_mode", ["exact", "fast"])
+@pytest.mark.parametrize("math_mode", ["exact", "fast", "approx"])
 def test_wavefront_tally_equals_history_tally(engine, cfg, math_mode):
     p = P.config2()[0]
     c = P.TallyConfig(500, 50.0, 50)
