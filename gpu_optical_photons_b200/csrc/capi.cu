@@ -10,6 +10,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <thread>
+#include <tuple>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -493,6 +496,99 @@ int engine_check_ctrl(optx_engine* e, WaveCtrl& c, cudaStream_t st) {
 
 }  // namespace
 
+// Records pipeline: chunk i's kernel runs on the compute stream while chunk
+// i-1's records stream to the host on the copy stream, double-buffered on the
+// device. Pinned caller arrays receive the DMA directly; pageable ones are
+// filled from cached pinned staging buffers by a multi-threaded host copy that
+// overlaps the next chunk's kernel (the reference copies synchronously into
+// pageable vectors, gpu_backend.cu:119-156, cuda_util.cuh:98-111).
+namespace {
+
+struct RecPipe {
+  uint64_t cap = 0;  // photons per buffer set
+  void* dev[2] = {nullptr, nullptr};
+  unsigned char* pin[2] = {nullptr, nullptr};
+  cudaStream_t comp = nullptr, copy = nullptr;
+  cudaEvent_t k0[2], k1[2], c1[2];
+  bool events = false;
+};
+RecPipe g_pipe;
+
+// Structure-of-arrays views of one buffer set of `cap` photons (256-B aligned arrays).
+template <class Ptr>
+void carve(unsigned char* base, uint64_t cap, Ptr& fate, Ptr (&w)[7]) {
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    unsigned char* q = base + off;
+    off += (b + 255) & ~size_t(255);
+    return q;
+  };
+  fate = take(cap);
+  for (int i = 0; i < 7; ++i) w[i] = take(cap * 4);
+}
+size_t set_bytes(uint64_t cap) { return cap + 7 * ((cap * 4 + 255) & ~size_t(255)) + 256; }
+
+int pipe_ensure(uint64_t cap) {
+  if (!g_pipe.events) {
+    OPTX_CUDA(cudaStreamCreateWithFlags(&g_pipe.comp, cudaStreamNonBlocking));
+    OPTX_CUDA(cudaStreamCreateWithFlags(&g_pipe.copy, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+      OPTX_CUDA(cudaEventCreate(&g_pipe.k0[b]));
+      OPTX_CUDA(cudaEventCreate(&g_pipe.k1[b]));
+      OPTX_CUDA(cudaEventCreate(&g_pipe.c1[b]));
+    }
+    g_pipe.events = true;
+  }
+  if (g_pipe.cap >= cap) return OPTX_OK;
+  for (int b = 0; b < 2; ++b) {
+    if (g_pipe.dev[b]) cudaFree(g_pipe.dev[b]);
+    if (g_pipe.pin[b]) cudaFreeHost(g_pipe.pin[b]);
+    g_pipe.dev[b] = nullptr;
+    g_pipe.pin[b] = nullptr;
+  }
+  g_pipe.cap = 0;
+  for (int b = 0; b < 2; ++b) {
+    OPTX_CUDA(cudaMalloc(&g_pipe.dev[b], set_bytes(cap)));
+    OPTX_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&g_pipe.pin[b]), set_bytes(cap),
+                            cudaHostAllocDefault));
+  }
+  g_pipe.cap = cap;
+  return OPTX_OK;
+}
+
+bool is_pinned(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// memcpy of large blocks split over a few host threads.
+void parallel_copy(const std::vector<std::tuple<void*, const void*, size_t>>& jobs) {
+  size_t total = 0;
+  for (auto& j : jobs) total += std::get<2>(j);
+  const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  if (total < (8u << 20) || hw == 1) {
+    for (auto& j : jobs) std::memcpy(std::get<0>(j), std::get<1>(j), std::get<2>(j));
+    return;
+  }
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < hw; ++t) {
+    th.emplace_back([&, t] {
+      for (auto& j : jobs) {
+        const size_t b = std::get<2>(j), lo = b * t / hw, hi = b * (t + 1) / hw;
+        std::memcpy(static_cast<char*>(std::get<0>(j)) + lo, static_cast<const char*>(std::get<1>(j)) + lo,
+                    hi - lo);
+      }
+    });
+  }
+  for (auto& x : th) x.join();
+}
+
+}  // namespace
+
 // =============================================================================
 extern "C" {
 
@@ -533,36 +629,92 @@ int optx_release_cache(void) {
 }
 
 int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
-                     const optx_records* out, int block_size, uint64_t first_id, uint64_t chunk,
-                     int math, optx_timing* timing) {
+                                const optx_records* out, int block_size, uint64_t first_id,
+                                uint64_t chunk, int math, optx_timing* timing) {
   std::lock_guard<std::mutex> lk(g_mu);
   OPTX_TRY(check_params(p, faces));
   OPTX_TRY(check_block(block_size));
   OPTX_TRY(check_math(math));
   if (n > 0) OPTX_TRY(check_records(out));
   OPTX_TRY(ensure_device());
-  OPTX_TRY(cache_events());
   optx_timing tm{};
   const auto t0 = std::chrono::steady_clock::now();
-  const DevParams P = make_dev_params(*p, faces);
-  const uint64_t cap = std::max<uint64_t>(1, std::min<uint64_t>(n, chunk ? chunk : (uint64_t{1} << 24)));
-  const auto ta = std::chrono::steady_clock::now();
-  DevRecords d{};
-  OPTX_TRY(cache_records(cap, d));
-  tm.alloc_ms = ms_since(ta);
-  for (uint64_t done = 0; done < n; done += cap) {
-    const uint64_t m = std::min(cap, n - done);
-    OPTX_CUDA(cudaEventRecord(g_cache.e0, 0));
-    OPTX_CUDA(DISPATCH(math, launch_history_records, P, first_id + done, m, d, block_size, nullptr));
-    OPTX_CUDA(cudaEventRecord(g_cache.e1, 0));
-    OPTX_CUDA(cudaEventSynchronize(g_cache.e1));
-    float ms = 0.f;
-    OPTX_CUDA(cudaEventElapsedTime(&ms, g_cache.e0, g_cache.e1));
-    tm.kernel_ms += ms;
-    const auto tc = std::chrono::steady_clock::now();
-    OPTX_TRY(copy_records_d2h(out, done, d, m));
-    tm.d2h_ms += ms_since(tc);
+  if (n == 0) {
+    if (timing) *timing = tm;
+    return OPTX_OK;
   }
+  const DevParams P = make_dev_params(*p, faces);
+  // `chunk` bounds the device memory as in the reference; the pipeline holds two
+  // buffer sets of at most 2^22 photons each within it.
+  const uint64_t cap = std::max<uint64_t>(
+      1, std::min<uint64_t>({n, chunk ? chunk : (uint64_t{1} << 24), uint64_t{1} << 22}));
+  const auto ta = std::chrono::steady_clock::now();
+  OPTX_TRY(pipe_ensure(cap));
+  tm.alloc_ms = ms_since(ta);
+  void* outs[8] = {out->fate, out->n_boundary, out->n_scatter, out->t, out->x, out->y, out->z, out->path};
+  bool direct = true;
+  for (void* q : outs) direct = direct && is_pinned(q);
+  const size_t elem[8] = {1, 4, 4, 4, 4, 4, 4, 4};
+  auto views = [&](int b, bool host) {
+    unsigned char* base = host ? g_pipe.pin[b] : static_cast<unsigned char*>(g_pipe.dev[b]);
+    unsigned char* fate;
+    unsigned char* w[7];
+    carve(base, cap, fate, w);
+    std::array<unsigned char*, 8> v{fate, w[0], w[1], w[2], w[3], w[4], w[5], w[6]};
+    return v;
+  };
+  const uint64_t chunks = (n + cap - 1) / cap;
+  float kms = 0.f, cms = 0.f;
+  auto host_fill = [&](uint64_t i) {  // staging set (i % 2) -> caller arrays
+    const uint64_t done = i * cap, m = std::min(cap, n - done);
+    auto src = views(static_cast<int>(i % 2), true);
+    std::vector<std::tuple<void*, const void*, size_t>> jobs;
+    for (int k = 0; k < 8; ++k)
+      jobs.emplace_back(static_cast<char*>(outs[k]) + done * elem[k], src[k], m * elem[k]);
+    parallel_copy(jobs);
+  };
+  for (uint64_t i = 0; i < chunks; ++i) {
+    const int b = static_cast<int>(i % 2);
+    const uint64_t done = i * cap, m = std::min(cap, n - done);
+    auto dv = views(b, false);
+    // the device set b is free once the copy of chunk i - 2 has finished
+    if (i >= 2) OPTX_CUDA(cudaStreamWaitEvent(g_pipe.comp, g_pipe.c1[b], 0));
+    OPTX_CUDA(cudaEventRecord(g_pipe.k0[b], g_pipe.comp));
+    const DevRecords d{dv[0], reinterpret_cast<uint32_t*>(dv[1]), reinterpret_cast<uint32_t*>(dv[2]),
+                       reinterpret_cast<float*>(dv[3]), reinterpret_cast<float*>(dv[4]),
+                       reinterpret_cast<float*>(dv[5]), reinterpret_cast<float*>(dv[6]),
+                       reinterpret_cast<float*>(dv[7])};
+    OPTX_CUDA(DISPATCH(math, launch_history_records, P, first_id + done, m, d, block_size, g_pipe.comp));
+    OPTX_CUDA(cudaEventRecord(g_pipe.k1[b], g_pipe.comp));
+    OPTX_CUDA(cudaStreamWaitEvent(g_pipe.copy, g_pipe.k1[b], 0));
+    auto hv = views(b, true);
+    for (int k = 0; k < 8; ++k) {
+      void* dst = direct ? static_cast<void*>(static_cast<char*>(outs[k]) + done * elem[k])
+                         : static_cast<void*>(hv[k]);
+      OPTX_CUDA(cudaMemcpyAsync(dst, dv[k], m * elem[k], cudaMemcpyDeviceToHost, g_pipe.copy));
+    }
+    OPTX_CUDA(cudaEventRecord(g_pipe.c1[b], g_pipe.copy));
+    if (i >= 1) {  // finish chunk i - 1 on the host while chunk i computes and copies
+      const int pb = static_cast<int>((i - 1) % 2);
+      OPTX_CUDA(cudaEventSynchronize(g_pipe.c1[pb]));
+      float ms = 0.f;
+      OPTX_CUDA(cudaEventElapsedTime(&ms, g_pipe.k0[pb], g_pipe.k1[pb]));
+      kms += ms;
+      OPTX_CUDA(cudaEventElapsedTime(&ms, g_pipe.k1[pb], g_pipe.c1[pb]));
+      cms += ms;
+      if (!direct) host_fill(i - 1);
+    }
+  }
+  const int lb = static_cast<int>((chunks - 1) % 2);
+  OPTX_CUDA(cudaEventSynchronize(g_pipe.c1[lb]));
+  float ms = 0.f;
+  OPTX_CUDA(cudaEventElapsedTime(&ms, g_pipe.k0[lb], g_pipe.k1[lb]));
+  kms += ms;
+  OPTX_CUDA(cudaEventElapsedTime(&ms, g_pipe.k1[lb], g_pipe.c1[lb]));
+  cms += ms;
+  if (!direct) host_fill(chunks - 1);
+  tm.kernel_ms = kms;
+  tm.d2h_ms = cms;  // kernel end to copy end per chunk (copies overlap later kernels)
   tm.total_ms = ms_since(t0);
   if (timing) *timing = tm;
   return OPTX_OK;

@@ -174,3 +174,25 @@ def test_edge_cases(engine):
         engine.run_gpu_records(p, 10, block_size=100)
     with pytest.raises(engine.OptxError):
         engine.run_gpu_tally(p, P.TallyConfig(100, 50.0, 300), 10)  # 360 KB of shared-memory bins
+
+
+def test_records_pipeline_pinned_and_pageable(engine):
+    """Multi-chunk records (several pipeline stages) equal one-shot device records, for
+    pageable numpy arrays and for pinned arrays (direct DMA)."""
+    import torch
+    p = P.config2()[0]
+    n = 9_000_001  # > 2 pipeline buffer sets of 2^22, ragged last chunk
+    d = engine.records_device(p, n, first_id=3)
+    torch.cuda.synchronize()
+    want = engine.records_to_numpy(d)
+    rec, tm = engine.run_gpu_records(p, n, first_id=3)
+    assert compare_histories(rec, want)["bitwise_identical"] == n
+    pinned = engine.Records()
+    for k in engine.Records.FIELDS:
+        dt = {"fate": torch.uint8, "n_boundary": torch.int32, "n_scatter": torch.int32}.get(k, torch.float32)
+        a = torch.empty(n, dtype=dt, pin_memory=True).numpy()
+        pinned[k] = a.view(np.uint32) if k in ("n_boundary", "n_scatter") else a
+    rec2, _ = engine.run_gpu_records(p, n, first_id=3, out=pinned)
+    assert compare_histories(rec2, want)["bitwise_identical"] == n
+    small, _ = engine.run_gpu_records(p, 1000, first_id=3, chunk=77)  # many tiny chunks
+    assert compare_histories(small, {k: v[:1000] for k, v in want.items()})["bitwise_identical"] == 1000
