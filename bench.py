@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--threshold", type=int, default=0, help="0: tuned default")
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--bps", type=int, default=0, help="resident blocks per SM (register budget)")
+    ap.add_argument("--chunk", type=int, default=0, help="photons a warp claims per grab (0: 256)")
     ap.add_argument("--no-autotune", action="store_true", help="use the default engine settings")
     ap.add_argument("--math", default="fast", choices=["fast", "exact", "approx"],
                     help="math mode of the kernels (see include/optx.h)")
@@ -216,9 +217,10 @@ def run_optx(args):
     first_id = shard_first_id(rank, n_photons)  # disjoint photon ids per rank
     tc = TallyConfig(100, 50.0, 10)
     cfg = WaveConfig(block_size=args.block or 256, threshold=args.threshold or 28,
-                     blocks_per_sm=args.bps or 3, use_graph=not args.host_loop, math=args.math)
+                     blocks_per_sm=args.bps or 3, use_graph=not args.host_loop, math=args.math,
+                     chunk=args.chunk)
     tuned = None
-    if not args.no_autotune and not args.host_loop and not (args.threshold or args.bps or args.block):
+    if not args.no_autotune and not args.host_loop and not (args.threshold or args.bps or args.block or args.chunk):
         from gpu_optical_photons_b200.autotune import tune
         t0 = time.perf_counter()
         cfg, tune_log = tune(events, counts, tc, base=cfg, repeats=2)
@@ -325,7 +327,8 @@ def run_optx(args):
                    "engine": {"block_size": cfg.block_size, "threshold": cfg.threshold,
                               "wave_quota": cfg.wave_quota,
                               "blocks_per_sm": cfg.blocks_per_sm,
-                              "cadence": cfg.cadence, "graph": cfg.use_graph, "math": cfg.math},
+                              "cadence": cfg.cadence, "chunk": cfg.chunk or 256,
+                              "graph": cfg.use_graph, "math": cfg.math},
                    "parallelism": f"dp{world} (independent event batches per GPU)"},
         "e2e": {"value": world * steps_per_run / (e2e_step * 1e-3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,

@@ -63,7 +63,8 @@ class CWaveConfig(ctypes.Structure):
     _fields_ = [("block_size", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
                 ("threshold", ctypes.c_uint32), ("cadence", ctypes.c_uint32),
                 ("wave_quota", ctypes.c_uint64), ("use_graph", ctypes.c_int32),
-                ("math", ctypes.c_int32)]
+                ("math", ctypes.c_int32), ("chunk", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 _P = ctypes.c_void_p

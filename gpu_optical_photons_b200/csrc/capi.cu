@@ -304,6 +304,9 @@ size_t wave_smem(const optx_engine* e, int mode, bool batch) {
   const size_t pantry = static_cast<size_t>(e->cfg.block_size / 32) * kPantryBytesPerWarp;
   if (mode == kModeTally && !batch) return pantry + static_cast<size_t>(e->tdev.len - 7u) * 4u;
   if (mode == kModeAdjoint) return pantry + static_cast<size_t>(e->tdev.time_bins + 1u) * 8u;
+  if (mode == kModeTally && batch)  // per-warp event slots
+    return pantry + static_cast<size_t>(e->cfg.block_size / 32) *
+                        (kSlotCounterBytesPerWarp + slot_bin_bytes_per_warp(e->tdev.len - 7u));
   return pantry;
 }
 
@@ -374,6 +377,7 @@ int engine_upload_args(optx_engine* e, int mode, bool batch, int grid, cudaGraph
       4ull * (max_steps + 2ull) + 4ull * (e->total / per_wave) + 64ull;
   a.wave_cap = static_cast<uint32_t>(std::min<unsigned long long>(std::max(cap, 100000ull), 0xfffffff0ull));
   a.use_graph = (e->cfg.use_graph >= 0) ? 1u : 0u;
+  a.chunk = e->cfg.chunk;
   (void)grid;
   (void)batch;
   OPTX_CUDA(cudaMemcpyAsync(e->d_args, &a, sizeof(a), cudaMemcpyHostToDevice, st));
@@ -847,6 +851,10 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
   if (k.threshold == 0) k.threshold = 28;
   if (k.threshold > 32) return fail(OPTX_ERR_INVALID_ARGUMENT, "threshold must be 1..32");
   if (k.use_graph == 0) k.use_graph = 1;
+  if (k.chunk == 0) k.chunk = 256;
+  if (k.chunk < 32 || k.chunk > (1u << 20))
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "chunk must be in [32, 2^20]");
+  if (k.reserved != 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "reserved must be 0");
   OPTX_TRY(check_math(k.math));
   OPTX_TRY(ensure_device());
   auto* e = new optx_engine();
@@ -1210,6 +1218,7 @@ extern "C" int optx_wavefront_tally_noalloc(const optx_params* p, const optx_fac
   a.tally = d_tally;
   a.tc = td;
   a.use_graph = 0u;
+  a.chunk = 256u;
   a.iter_cap = (static_cast<unsigned long long>(n) + a.qcap + 64ull) * (P.max_steps + 2ull) + 4096ull;
   a.wave_cap = static_cast<uint32_t>(std::min<unsigned long long>(
       std::max<unsigned long long>(4ull * (P.max_steps + 2ull) + 64ull, 100000ull), 0xfffffff0ull));

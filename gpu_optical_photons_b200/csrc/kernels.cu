@@ -226,11 +226,15 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
   const uint32_t warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
   const uint32_t nwarps = blockDim.x >> 5;
-  // [pantries: nwarps x 32 x 112 B][block histograms (tally) or bin weights (adjoint)]
+  // [pantries: nwarps x 32 x 112 B][block histograms (tally), bin weights (adjoint)
+  //  or, batched tally, per-warp event slots: nwarps x 2 x 8 u64 counters, then
+  //  nwarps x 2 x n_bins u32 bins when n_bins <= kSlotBins]
+  constexpr bool kSlots = BATCH && MODE == kModeTally;
   float4* pantry = reinterpret_cast<float4*>(smem_raw + warp * kPantryBytesPerWarp);
   unsigned char* extra = smem_raw + nwarps * kPantryBytesPerWarp;
   uint32_t* s_hist = reinterpret_cast<uint32_t*>(extra);
   double* s_w = reinterpret_cast<double*>(extra);
+  unsigned long long* s_evc = reinterpret_cast<unsigned long long*>(extra) + warp * 16u;
   __shared__ double s_red[4][16];
 
   // Wave-constant values live in shared memory, not in each thread's registers.
@@ -238,7 +242,7 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
     const float4* qin;
     float4* qout;
     unsigned long long fresh_next, first_id, iter_cap;
-    uint32_t n_in, items, T, cadence, qcap;
+    uint32_t n_in, items, T, cadence, qcap, chunk;
     TallyDev tc;
   };
   __shared__ WaveShared ws;
@@ -254,6 +258,7 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
     ws.qcap = A->qcap;
     ws.first_id = A->first_id;
     ws.iter_cap = A->iter_cap;
+    ws.chunk = A->chunk < 32u ? 32u : A->chunk;
     ws.tc = A->tc;
   }
   __syncthreads();
@@ -265,10 +270,21 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
   const uint32_t& qcap = ws.qcap;
   const unsigned long long& first_id = ws.first_id;
   const unsigned long long& iter_cap = ws.iter_cap;
+  const uint32_t& wchunk = ws.chunk;
   const TallyDev& tc = ws.tc;
+  const uint32_t n_bins = tc.len - 7u;
+  const bool slot_bins = n_bins <= kSlotBins;
+  uint32_t* s_sb = reinterpret_cast<uint32_t*>(extra + nwarps * kSlotCounterBytesPerWarp) +
+                   warp * 2u * n_bins;  // this warp's [2][n_bins] (when slot_bins)
 
   if (MODE == kModeTally && !BATCH) {
-    for (uint32_t b = threadIdx.x; b < tc.len - 7u; b += blockDim.x) s_hist[b] = 0u;
+    for (uint32_t b = threadIdx.x; b < n_bins; b += blockDim.x) s_hist[b] = 0u;
+  }
+  if (kSlots) {
+    if (lane < 16u) s_evc[lane] = 0ull;
+    if (slot_bins) {
+      for (uint32_t b = lane; b < 2u * n_bins; b += 32u) s_sb[b] = 0u;
+    }
   }
   if (MODE == kModeAdjoint) {
     for (uint32_t b = threadIdx.x; b <= tc.time_bins; b += blockDim.x) s_w[b] = A->w_bin[b];
@@ -284,34 +300,75 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
   bool refilled = false;   // warp-uniform: lanes were loaded and have not stepped yet
   uint32_t pc = 0u;        // warp-uniform: photons waiting in this warp's pantry
   uint32_t wsteps = 0u;
-  // Per-lane tallies (flushed at the end; batched: when the lane's event changes).
+  // Work items [chunk_lo, chunk_hi) claimed by this warp and not yet emitted (warp-uniform).
+  uint32_t chunk_lo = 0u, chunk_hi = 0u;
+  // Single configuration: per-lane tallies, flushed at the end of the wave.
   uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0, snb = 0, sns = 0;
-  uint32_t cur_ev = 0xffffffffu;
+  // Batched: the events cached in this warp's two shared-memory slots (warp-uniform).
+  constexpr uint32_t kNoEvent = 0xffffffffu;
+  uint32_t tag0 = kNoEvent, tag1 = kNoEvent, victim = 0u;
   double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
   uint32_t useful = 0u, iters = 0u;
 
-  auto flush_event = [&]() {
-    if (cur_ev == 0xffffffffu) return;
-    unsigned long long* T0 = A->tally + static_cast<size_t>(cur_ev) * tc.len;
-    if (f0) atomicAdd(&T0[0], static_cast<unsigned long long>(f0));
-    if (f1) atomicAdd(&T0[1], static_cast<unsigned long long>(f1));
-    if (f2) atomicAdd(&T0[2], static_cast<unsigned long long>(f2));
-    if (f3) atomicAdd(&T0[3], static_cast<unsigned long long>(f3));
-    if (f4) atomicAdd(&T0[4], static_cast<unsigned long long>(f4));
-    if (snb) atomicAdd(&T0[tc.len - 2u], static_cast<unsigned long long>(snb));
-    if (sns) atomicAdd(&T0[tc.len - 1u], static_cast<unsigned long long>(sns));
-    f0 = f1 = f2 = f3 = f4 = snb = sns = 0u;
+  // Warp-collective: adds slot v's counters and bins to event `tag`'s tally
+  // slice and clears the slot.
+  auto flush_slot = [&](uint32_t v, uint32_t tag) {
+    __syncwarp();
+    if (tag != kNoEvent) {
+      unsigned long long* G = A->tally + static_cast<size_t>(tag) * tc.len;
+      if (lane < 7u) {  // 5 fates, then the nb and ns sums (the last two entries)
+        const unsigned long long c = s_evc[v * 8u + lane];
+        if (c != 0ull) {
+          atomicAdd(&G[lane < 5u ? lane : tc.len - 7u + lane], c);
+          s_evc[v * 8u + lane] = 0ull;
+        }
+      }
+      if (slot_bins) {
+        uint32_t* sb = s_sb + v * n_bins;
+        for (uint32_t b = lane; b < n_bins; b += 32u) {
+          const uint32_t c = sb[b];
+          if (c != 0u) {
+            atomicAdd(&G[5u + b], static_cast<unsigned long long>(c));
+            sb[b] = 0u;
+          }
+        }
+      }
+    }
+    __syncwarp();
   };
 
   // Bookkeeping of a finished photon.
   auto finish = [&](uint32_t fate, const DevParams& P) {
     if (MODE == kModeRecords) {
       store_record(A->rec, pidx, s, fate);
-    } else if (MODE == kModeTally) {
-      if (BATCH && ev != cur_ev) {
-        flush_event();
-        cur_ev = ev;
+    } else if (MODE == kModeTally && BATCH) {
+      // Shared-memory atomics into the event's slot when the warp caches it,
+      // else global atomics into the event's slice.
+      const int slot = ev == tag0 ? 0 : (ev == tag1 ? 1 : -1);
+      unsigned long long* G = A->tally + static_cast<size_t>(ev) * tc.len;
+      if (slot >= 0) {
+        unsigned long long* C = s_evc + slot * 8;
+        atomicAdd(&C[fate], 1ull);
+        if (s.nb) atomicAdd(&C[5], static_cast<unsigned long long>(s.nb));
+        if (s.ns) atomicAdd(&C[6], static_cast<unsigned long long>(s.ns));
+      } else {
+        atomicAdd(&G[fate], 1ull);
+        if (s.nb) atomicAdd(&G[tc.len - 2u], static_cast<unsigned long long>(s.nb));
+        if (s.ns) atomicAdd(&G[tc.len - 1u], static_cast<unsigned long long>(s.ns));
       }
+      if (fate == kDetected) {
+        const uint32_t tb = time_bin(s.t, tc.tscale, tc.time_bins);
+        const uint32_t xb = tc.time_bins + 1u + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins);
+        if (slot >= 0 && slot_bins) {
+          uint32_t* sb = s_sb + static_cast<uint32_t>(slot) * n_bins;
+          atomicAdd(&sb[tb], 1u);
+          atomicAdd(&sb[xb], 1u);
+        } else {
+          atomicAdd(&G[5u + tb], 1ull);
+          atomicAdd(&G[5u + xb], 1ull);
+        }
+      }
+    } else if (MODE == kModeTally) {
       f0 += fate == 0u;
       f1 += fate == 1u;
       f2 += fate == 2u;
@@ -320,27 +377,15 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
       // Per-lane step sums stay far below 2^31 between flushes (a lane sees at
       // most wave_quota / lanes photons of max_steps steps); flush early if not.
       if (snb > 0x7fffffffu || sns > 0x7fffffffu) {
-        if (BATCH) {
-          flush_event();
-        } else {
-          atomicAdd(&A->tally[tc.len - 2u], static_cast<unsigned long long>(snb));
-          atomicAdd(&A->tally[tc.len - 1u], static_cast<unsigned long long>(sns));
-          snb = sns = 0u;
-        }
+        atomicAdd(&A->tally[tc.len - 2u], static_cast<unsigned long long>(snb));
+        atomicAdd(&A->tally[tc.len - 1u], static_cast<unsigned long long>(sns));
+        snb = sns = 0u;
       }
       snb += s.nb;
       sns += s.ns;
       if (fate == kDetected) {
-        const uint32_t tb = time_bin(s.t, tc.tscale, tc.time_bins);
-        const uint32_t xb = tc.time_bins + 1u + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins);
-        if (BATCH) {
-          unsigned long long* T0 = A->tally + static_cast<size_t>(ev) * tc.len + 5u;
-          atomicAdd(&T0[tb], 1ull);
-          atomicAdd(&T0[xb], 1ull);
-        } else {
-          atomicAdd(&s_hist[tb], 1u);
-          atomicAdd(&s_hist[xb], 1u);
-        }
+        atomicAdd(&s_hist[time_bin(s.t, tc.tscale, tc.time_bins)], 1u);
+        atomicAdd(&s_hist[tc.time_bins + 1u + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins)], 1u);
       }
     } else {  // adjoint: score terms of detected photons (see WaveArgs)
       if (fate == kDetected) {
@@ -395,19 +440,35 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
       const uint32_t need = 32u - na;
       if (pc < need && !exhausted) {
         // Refill the pantry: all lanes emit (or load) one photon each together,
-        // so emission code runs on full warps.
+        // so emission code runs on full warps. Items come from the warp's claimed
+        // chunk of consecutive items, then from a newly claimed chunk (one atomic
+        // per `chunk` items keeps a warp on one event for many photons).
         const uint32_t room = 32u - pc;
-        uint32_t base = 0u;
-        if (lane == 0u) base = atomicAdd(&ctrl->cursor, room);
-        base = __shfl_sync(kFull, base, 0);
-        const uint32_t got = base >= items ? 0u : min(room, items - base);
+        const uint32_t base1 = chunk_lo;
+        const uint32_t got1 = min(room, chunk_hi - chunk_lo);
+        chunk_lo += got1;
+        uint32_t base2 = 0u, got = got1;
+        if (got1 < room) {
+          unsigned long long b = 0ull;
+          if (lane == 0u) b = atomicAdd(&ctrl->cursor, static_cast<unsigned long long>(wchunk));
+          b = __shfl_sync(kFull, b, 0);
+          const unsigned long long hi = b + wchunk;
+          chunk_lo = b < items ? static_cast<uint32_t>(b) : items;
+          chunk_hi = hi < items ? static_cast<uint32_t>(hi) : items;
+          const uint32_t got2 = min(room - got1, chunk_hi - chunk_lo);
+          base2 = chunk_lo;
+          chunk_lo += got2;
+          got += got2;
+        }
+        // A fresh chunk holds >= 32 items unless the wave's items ran out.
         exhausted = got < room;
+        uint32_t nev = 0u;
         if (lane < got) {
-          const uint32_t item = base + lane;
+          const uint32_t item = lane < got1 ? base1 + lane : base2 + (lane - got1);
           Photon ns{};
           Rng nr{};
           ScoreAux na_aux{0u, 0.0f};
-          uint32_t npidx, nev = 0u;
+          uint32_t npidx;
           if (item < n_in) {
             // A survivor of the previous wave: 4 x 128-bit loads from its tile.
             const float4* q = ws.qin + qidx(item);
@@ -447,6 +508,18 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
           }
         }
         pc += got;
+        if (kSlots && got > 0u) {
+          // Cache the newest event in a slot; keep the slot of the oldest event
+          // of this refill if it has one, else replace the slots in turn.
+          const uint32_t e_first = __shfl_sync(kFull, nev, 0);
+          const uint32_t e_last = __shfl_sync(kFull, nev, got - 1u);
+          if (e_last != tag0 && e_last != tag1) {
+            const uint32_t v = tag0 == e_first ? 1u : (tag1 == e_first ? 0u : victim);
+            victim = v ^ 1u;
+            flush_slot(v, v == 0u ? tag0 : tag1);
+            if (v == 0u) tag0 = e_last; else tag1 = e_last;
+          }
+        }
         __syncwarp();
       }
       if (pc > 0u) {
@@ -528,7 +601,8 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
   }
   if (MODE == kModeTally) {
     if (BATCH) {
-      flush_event();
+      flush_slot(0u, tag0);
+      flush_slot(1u, tag1);
     } else {
       const uint32_t r0 = __reduce_add_sync(kFull, f0), r1 = __reduce_add_sync(kFull, f1),
                      r2 = __reduce_add_sync(kFull, f2), r3 = __reduce_add_sync(kFull, f3),

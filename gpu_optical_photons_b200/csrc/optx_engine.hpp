@@ -47,6 +47,8 @@ struct WaveArgs {
   unsigned long long iter_cap;          // watchdog: max loop iterations per warp per wave
   uint32_t use_graph;                   // 1: the wave loop is a graph while node (set its condition)
   uint32_t wave_cap;                    // watchdog: max waves per run
+  uint32_t chunk;                       // consecutive work items a warp claims per grab (>= 32)
+  uint32_t pad2;
 };
 
 // Dynamic state of a wavefront run (device memory).
@@ -54,16 +56,15 @@ struct WaveCtrl {
   unsigned long long fresh_next;   // first fresh photon (relative index) of the current wave
   unsigned long long useful;       // lane-steps that advanced a photon
   unsigned long long issued;       // 32 x warp step iterations
+  unsigned long long cursor;       // work items claimed (atomic; may run past the wave's items)
   unsigned int wave;               // current wave number
   unsigned int n_in;               // survivors carried into the current wave
   unsigned int fresh_count;        // fresh photons admitted in the current wave
-  unsigned int cursor;             // work items handed out (atomic)
   unsigned int n_out;              // survivors spilled (atomic)
   unsigned int blocks_done;        // blocks finished (atomic)
   unsigned int active;             // 0 once the run is complete
   unsigned int error;              // bit 0 queue overflow, bit 1 watchdog
   unsigned int spills;             // total photons spilled over the run
-  unsigned int pad;
 };
 
 enum WaveMode : int { kModeTally = 0, kModeRecords = 1, kModeAdjoint = 2 };
@@ -72,6 +73,14 @@ constexpr uint32_t kEvShift = 7;  // event lookup table: one entry per 128 photo
 // the 112-byte stride makes 8 lanes' 128-bit accesses hit 8 distinct bank groups).
 constexpr uint32_t kPantryBytesPerWarp = 32u * 112u;
 constexpr unsigned kErrQueue = 1u, kErrWatchdog = 2u;
+// Batched tallies: each warp caches the counters of two events in shared memory
+// (7 x u64 per event, padded to 8) and, when the tally has at most kSlotBins
+// histogram bins, their time / hit-map bins too (u32).
+constexpr uint32_t kSlotBins = 256u;
+constexpr uint32_t kSlotCounterBytesPerWarp = 2u * 8u * 8u;
+inline __host__ __device__ uint32_t slot_bin_bytes_per_warp(uint32_t n_bins) {
+  return n_bins <= kSlotBins ? 2u * n_bins * 4u : 0u;
+}
 
 #define OPTX_DECLARE_LAUNCHERS(NS)                                                               \
   namespace NS {                                                                                 \

@@ -28,10 +28,12 @@ class WaveConfig:
     wave_quota: int = 0         # fresh photons per wave (0 = all)
     use_graph: bool = True
     math: str = "fast"
+    chunk: int = 0              # consecutive photons a warp claims per grab (0 = 256)
 
     def to_c(self) -> _lib.CWaveConfig:
         return _lib.CWaveConfig(self.block_size, self.blocks_per_sm, self.threshold, self.cadence,
-                                self.wave_quota, 1 if self.use_graph else -1, _lib.MATH[self.math])
+                                self.wave_quota, 1 if self.use_graph else -1, _lib.MATH[self.math],
+                                self.chunk, 0)
 
 
 def _events_c(events):

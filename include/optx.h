@@ -102,7 +102,10 @@ typedef struct optx_wave_config {
   uint32_t cadence;      /* steps per photon per wave before a forced spill, 0 = none (default 0) */
   uint64_t wave_quota;   /* fresh photons admitted per wave, 0 = all (default) */
   int32_t use_graph;     /* 1: waves run as a CUDA-graph while loop (default); -1: host loop */
-  int32_t math;          /* OPTX_MATH_FAST / OPTX_MATH_EXACT */
+  int32_t math;          /* OPTX_MATH_FAST / OPTX_MATH_EXACT / OPTX_MATH_APPROX */
+  uint32_t chunk;        /* consecutive photons a warp claims per grab, 32..2^20 (default 256);
+                            results do not depend on it */
+  uint32_t reserved;     /* must be 0 */
 } optx_wave_config;
 
 /* ---- device ---------------------------------------------------------- */

@@ -57,7 +57,7 @@ def test_struct_layouts():
     assert ctypes.sizeof(_lib.CRecords) == 64
     assert ctypes.sizeof(_lib.CTiming) == 40
     assert ctypes.sizeof(_lib.CEventStats) == 40
-    assert ctypes.sizeof(_lib.CWaveConfig) == 32
+    assert ctypes.sizeof(_lib.CWaveConfig) == 40
 
 
 def test_invalid_arguments_raise_value_error(lib):

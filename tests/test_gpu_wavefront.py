@@ -81,6 +81,30 @@ def test_batched_events_exact_equals_oracle(engine, oracle):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("chunk", [32, 33, 1000, 65536])
+@pytest.mark.parametrize("bins", [(100, 10), (300, 12)])  # bins cached per warp / global bins
+def test_batched_tallies_independent_of_chunk(engine, oracle, chunk, bins):
+    events, counts = batched_events(n_events=40, seed=19, median=3000, n_min=1, n_max=30000)
+    counts[5] = 0
+    c = P.TallyConfig(bins[0], 50.0, bins[1])
+    eng = WavefrontEngine(c, len(events), int(counts.sum()),
+                          WaveConfig(math="exact", threshold=26, chunk=chunk))
+    eng.set_events(events, counts)
+    eng.run_tally()
+    got = eng.tallies()
+    eng.close()
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
+    arr = (P.CSimParams * len(events))(*[e.to_c() for e in events])
+    assert np.array_equal(got, oracle.batch_tally(arr, offs, c, mode=oracle.PORTABLE))
+
+
+def test_chunk_out_of_range_rejected(engine):
+    from gpu_optical_photons_b200._lib import InvalidArgument
+    for chunk in (16, (1 << 20) + 1):
+        with pytest.raises(InvalidArgument):
+            WavefrontEngine(P.TallyConfig(), 1, 100, WaveConfig(chunk=chunk))
+
+
 def test_batched_events_fast_vs_oracle(engine, oracle):
     events, counts = batched_events(n_events=64, seed=11, median=5000)
     c = P.TallyConfig(100, 50.0, 10)
