@@ -1082,8 +1082,17 @@ int optx_run_records_event(const optx_params* p, const optx_faces* faces, uint64
   optx_tally_config tc{1u, 1.0f, 1u};
   optx_wave_config cfg{};
   cfg.block_size = std::min(block_size, 256);  // launch geometry only; records do not depend on it
-  cfg.threshold = 32;
-  cfg.cadence = steps_per_launch >= p->max_steps ? 0u : steps_per_launch;
+  if (steps_per_launch >= p->max_steps) {
+    // One launch, history style (gpu_event.cu with k >= max_steps): each warp
+    // claims photons 32w .. 32w + 31 and runs until all have finished, so the
+    // issued lane-steps are 32 x the longest history of each such group.
+    cfg.threshold = 1;
+    cfg.chunk = 32;
+    cfg.cadence = 0;
+  } else {
+    cfg.threshold = 32;
+    cfg.cadence = steps_per_launch;
+  }
   cfg.use_graph = 1;
   cfg.math = math;
   optx_engine* e = nullptr;

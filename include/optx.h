@@ -138,8 +138,11 @@ int optx_run_tally(const optx_params* p, const optx_faces* faces, const optx_tal
  *   uint32_t steps_per_launch, int block_size = 256, uint64_t first_id = 0,
  *   uint64_t chunk = 1 << 24, EventStats* = nullptr) (backend.hpp:110-115;
  *   gpu_event.cu:174-244). Runs the wavefront engine with cadence = steps_per_launch:
- *   each photon advances at most that many steps per wave. Records are bit-identical
- *   to optx_run_records for every steps_per_launch, block_size and chunk. */
+ *   each photon advances at most that many steps per wave. With steps_per_launch >=
+ *   max_steps it runs one wave history style, as the reference's single launch: each
+ *   warp holds photons 32w .. 32w + 31 until all have finished, so issued_lane_steps =
+ *   sum over groups of 32 x the longest history. Records are bit-identical to
+ *   optx_run_records for every steps_per_launch, block_size and chunk. */
 int optx_run_records_event(const optx_params* p, const optx_faces* faces, uint64_t n,
                            const optx_records* out, uint32_t steps_per_launch, int block_size,
                            uint64_t first_id, uint64_t chunk, int math, optx_event_stats* stats,
