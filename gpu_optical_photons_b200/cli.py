@@ -35,9 +35,16 @@ def main(argv=None):
     ap.add_argument("--cadence", type=int, default=0)
     ap.add_argument("--host-loop", action="store_true", help="launch waves from the host (no graph)")
     ap.add_argument("--repeat", type=int, default=3)
+    ap.add_argument("--out", help="write records / tally .npy files and meta.json here "
+                    "(the reference's optphot --out layout)")
+    ap.add_argument("--time_bins", type=int)
+    ap.add_argument("--time_max", type=float)
+    ap.add_argument("--xy_bins", type=int)
     for key in ("n_scint", "n_det", "n_out", "abs_length", "scat_length", "reflectivity", "tau",
                 "src_x", "src_y", "src_z"):
         ap.add_argument(f"--{key}", type=float)
+    ap.add_argument("--surface", choices=sorted(P.SURFACE_NAMES))
+    ap.add_argument("--source", choices=["point", "volume"])
     ap.add_argument("--seed", type=int)
     ap.add_argument("--max_steps", type=int)
     a = ap.parse_args(argv)
@@ -52,6 +59,14 @@ def main(argv=None):
         v = getattr(a, key)
         if v is not None:
             setattr(p, key, v)
+    if a.surface is not None:
+        p.surface = P.SURFACE_NAMES[a.surface]
+    if a.source is not None:
+        p.source = P.POINT if a.source == "point" else P.VOLUME
+    for key in ("time_bins", "time_max", "xy_bins"):
+        v = getattr(a, key)
+        if v is not None:
+            setattr(c, key, v)
     n = int(a.n)
     out = {"config": a.config, "engine": a.engine, "mode": a.mode, "n": n, "math": a.math,
            "device": g.gpu_device_name()}
@@ -78,6 +93,10 @@ def main(argv=None):
             r = g.records_to_numpy(rec)
             flat = None
             out["steps"] = int(r.steps().sum())
+            if a.out:
+                from . import io
+                meta = io.params_to_json(p, io.RunOptions("gpu", "records", n, 1, a.block, c))
+                io.write_records(a.out, r, meta)
     else:
         cfg = WaveConfig(block_size=a.block, threshold=a.threshold, cadence=a.cadence,
                          use_graph=not a.host_loop, math=a.math)
@@ -96,6 +115,10 @@ def main(argv=None):
         t = g.Tally.from_flat(flat, c)
         out["fates"] = [int(v) for v in t.fate_counts]
         out["steps"] = t.steps()
+        if a.out:
+            from . import io
+            meta = io.params_to_json(p, io.RunOptions("gpu", "tally", n, 1, a.block, c))
+            io.write_tally(a.out, t, meta)
     best = min(times)
     out["ms"] = best
     out["photons_per_s"] = n / (best * 1e-3)

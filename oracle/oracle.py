@@ -83,6 +83,19 @@ def ref(mode: int = PLATFORM):
         L.ref_philox.argtypes = [_P, _P, _P]
         L.ref_max_threads.restype = ctypes.c_int
         L.ref_portable_math.restype = ctypes.c_int
+        L.ref_params_to_json.restype = ctypes.c_int
+        L.ref_params_to_json.argtypes = [_P, ctypes.c_char_p, ctypes.c_char_p, _u64, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32,
+                                         ctypes.c_char_p, ctypes.c_size_t]
+        L.ref_write_records.restype = ctypes.c_int
+        L.ref_write_records.argtypes = [ctypes.c_char_p, _u64] + [_P] * 8 + [ctypes.c_char_p]
+        L.ref_write_tally.restype = ctypes.c_int
+        L.ref_write_tally.argtypes = [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, _P,
+                                      ctypes.c_char_p]
+        L.ref_compare_json.restype = ctypes.c_int
+        L.ref_compare_json.argtypes = ([_u64] + [_P] * 8 + [_u64] + [_P] * 8 +
+                                       [_P, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                        ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t])
         _ref[mode] = L
     return _ref[mode]
 
@@ -214,6 +227,50 @@ def ref_philox(ctr, key, mode: int = PLATFORM) -> np.ndarray:
     out = np.zeros(4, np.uint32)
     ref(mode).ref_philox(_ptr(c), _ptr(k), _ptr(out))
     return out
+
+
+def _rec_ptrs(r):
+    arrs = [np.ascontiguousarray(r[k], dtype=dt) for k, dt in
+            zip(Records.FIELDS, (np.uint8, np.uint32, np.uint32) + (np.float32,) * 5)]
+    return arrs, [_ptr(a) for a in arrs]
+
+
+def ref_params_to_json(p, backend="gpu", mode="records", n_photons=1_000_000, threads=1,
+                       block_size=256, time_bins=100, time_max=50.0, xy_bins=50) -> str:
+    """The reference's params_to_json (src/core/config.cpp:230-253)."""
+    cp = p.to_c()
+    buf = ctypes.create_string_buffer(8192)
+    n = ref().ref_params_to_json(ctypes.byref(cp), backend.encode(), mode.encode(), n_photons, threads,
+                                 block_size, time_bins, time_max, xy_bins, buf, len(buf))
+    assert n >= 0
+    return buf.value.decode()
+
+
+def ref_write_records(directory: str, rec, meta: str) -> None:
+    """The reference's write_records (src/core/io.cpp:48-60)."""
+    keep, ptrs = _rec_ptrs(rec)
+    rc = ref().ref_write_records(directory.encode(), len(keep[0]), *ptrs, meta.encode())
+    assert rc == 0
+
+
+def ref_write_tally(directory: str, c, flat, meta: str) -> None:
+    """The reference's write_tally (src/core/io.cpp:62-72)."""
+    f = np.ascontiguousarray(flat, dtype=np.uint64)
+    assert ref().ref_write_tally(directory.encode(), c.time_bins, c.xy_bins, _ptr(f), meta.encode()) == 0
+
+
+def ref_compare_json(a, b, p, time_bins=100, t_max=0.0, xy_bins=20):
+    """(to_json(compare_histories(a, b)), to_json(compare_distributions(a, b, p, ...)))
+    of the reference (src/core/compare.cpp); the first is "null" for different sizes."""
+    ka, pa = _rec_ptrs(a)
+    kb, pb = _rec_ptrs(b)
+    cp = p.to_c()
+    h = ctypes.create_string_buffer(4096)
+    d = ctypes.create_string_buffer(4096)
+    rc = ref().ref_compare_json(len(ka[0]), *pa, len(kb[0]), *pb, ctypes.byref(cp), time_bins, t_max,
+                                xy_bins, h, d, len(h))
+    assert rc == 0
+    return h.value.decode(), d.value.decode()
 
 
 def compare_histories(a: Records, b: Records) -> dict:
