@@ -64,7 +64,15 @@ class CWaveConfig(ctypes.Structure):
                 ("threshold", ctypes.c_uint32), ("cadence", ctypes.c_uint32),
                 ("wave_quota", ctypes.c_uint64), ("use_graph", ctypes.c_int32),
                 ("math", ctypes.c_int32), ("chunk", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("max_gensteps", ctypes.c_uint32)]
+
+
+class CGenstep(ctypes.Structure):
+    """optx_genstep: 40 bytes."""
+    _fields_ = [("x0", ctypes.c_float), ("y0", ctypes.c_float), ("z0", ctypes.c_float),
+                ("t0", ctypes.c_float), ("x1", ctypes.c_float), ("y1", ctypes.c_float),
+                ("z1", ctypes.c_float), ("t1", ctypes.c_float), ("n_photons", ctypes.c_uint32),
+                ("event", ctypes.c_uint32)]
 
 
 _P = ctypes.c_void_p
@@ -94,6 +102,8 @@ _SIGS = {
     "optx_engine_get_tallies": [_P, _P, _P],
     "optx_engine_stats": [_P, _P, _P],
     "optx_run_batch": [_P, _P, _P, _P, ctypes.c_uint32, _u64, _P, _P, _P],
+    "optx_engine_set_gensteps": [_P, _P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, _u64, _P],
+    "optx_run_gensteps": [_P, _P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, _u64, _P, _P, _P],
 }
 
 

@@ -260,8 +260,10 @@ struct optx_engine {
   optx_wave_config cfg{};
   optx_tally_config tcfg{};
   TallyDev tdev{};
-  uint32_t max_events = 0;
+  uint32_t max_events = 0;   // tally slices
+  uint32_t max_records = 0;  // parameter records (events, or gensteps)
   uint64_t max_photons = 0;
+  uint64_t ev_entries = 0;   // capacity of the photon -> record table
   int n_sm = 0;
   size_t smem_tally = 0, smem_tally_batch = 0, smem_adj = 0;
   uint32_t qcap = 0;
@@ -271,13 +273,18 @@ struct optx_engine {
   DevParams* d_params = nullptr;
   unsigned long long* d_offsets = nullptr;
   uint32_t* d_evtable = nullptr;
+  uint32_t* d_tally_of = nullptr;  // genstep -> event (gensteps only)
+  float4* d_seg = nullptr;         // genstep segment ends and time windows
   float4* d_qa = nullptr;
   float4* d_qb = nullptr;
   unsigned long long* d_tally = nullptr;
   double* d_grad = nullptr;
   double* d_wbin = nullptr;
-  // current batch
+  // current batch: n_events records (events or gensteps) adding to n_tallies slices
   uint32_t n_events = 0;
+  uint32_t n_tallies = 0;
+  uint32_t ev_shift = kEvShift;
+  bool gensteps = false;
   uint64_t total = 0;
   uint64_t first_id = 0;
   DevParams P0{};
@@ -338,6 +345,10 @@ int engine_upload_args(optx_engine* e, int mode, bool batch, int grid, cudaGraph
   a.offsets = e->d_offsets;
   a.ev_table = e->d_evtable;
   a.n_events = e->n_events;
+  a.n_tallies = e->n_tallies;
+  a.ev_shift = e->ev_shift;
+  a.tally_of = e->gensteps ? e->d_tally_of : nullptr;
+  a.seg = e->gensteps ? e->d_seg : nullptr;
   a.threshold = e->cfg.threshold;
   a.cadence = e->cfg.cadence;
   a.qcap = e->qcap;
@@ -455,7 +466,8 @@ int engine_graph(optx_engine* e, int mode, bool batch, int grid, optx_engine::Gr
 int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_bin, double w_det,
                const double* theta_inv, uint32_t score_mask, cudaStream_t st) {
   if (e->n_events == 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "no events uploaded");
-  const bool batch = e->n_events > 1;
+  // Gensteps always run batched: each lane reads its genstep's record.
+  const bool batch = e->n_events > 1 || e->gensteps;
   int grid = 0;
   OPTX_TRY(engine_grid(e, mode, batch, grid));
   const size_t smem = wave_smem(e, mode, batch);
@@ -854,7 +866,7 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
   if (k.chunk == 0) k.chunk = 256;
   if (k.chunk < 32 || k.chunk > (1u << 20))
     return fail(OPTX_ERR_INVALID_ARGUMENT, "chunk must be in [32, 2^20]");
-  if (k.reserved != 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "reserved must be 0");
+  if (k.max_gensteps > (1u << 30)) return fail(OPTX_ERR_INVALID_ARGUMENT, "max_gensteps must be <= 2^30");
   OPTX_TRY(check_math(k.math));
   OPTX_TRY(ensure_device());
   auto* e = new optx_engine();
@@ -862,7 +874,11 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
   e->tcfg = *c;
   e->tdev = td;
   e->max_events = max_events;
+  e->max_records = std::max(max_events, k.max_gensteps);
   e->max_photons = max_photons;
+  // One table entry per 128 photons at least; finer (down to one per photon)
+  // when records are small and the table has room: 2 entries per record.
+  e->ev_entries = (max_photons >> kEvShift) + 2ull + 2ull * e->max_records;
   e->n_sm = num_sms();
   auto cleanup = [&](int rc) {
     optx_engine_destroy(e);
@@ -893,9 +909,13 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
   int rc = OPTX_OK;
   if ((rc = alloc(reinterpret_cast<void**>(&e->d_args), sizeof(WaveArgs))) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_ctrl), sizeof(WaveCtrl))) ||
-      (rc = alloc(reinterpret_cast<void**>(&e->d_params), sizeof(DevParams) * max_events)) ||
-      (rc = alloc(reinterpret_cast<void**>(&e->d_offsets), 8ull * (max_events + 1ull))) ||
-      (rc = alloc(reinterpret_cast<void**>(&e->d_evtable), 4ull * ((max_photons >> kEvShift) + 2ull))) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_params), sizeof(DevParams) * e->max_records)) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_offsets), 8ull * (e->max_records + 1ull))) ||
+      (rc = alloc(reinterpret_cast<void**>(&e->d_evtable), 4ull * e->ev_entries)) ||
+      (k.max_gensteps > 0 &&
+       (rc = alloc(reinterpret_cast<void**>(&e->d_tally_of), 4ull * k.max_gensteps))) ||
+      (k.max_gensteps > 0 &&
+       (rc = alloc(reinterpret_cast<void**>(&e->d_seg), 32ull * k.max_gensteps))) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_qa), qcap * 64ull)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_qb), qcap * 64ull)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_tally), 8ull * td.len * max_events)) ||
@@ -919,6 +939,8 @@ int optx_engine_destroy(optx_engine* e) {
   cudaFree(e->d_params);
   cudaFree(e->d_offsets);
   cudaFree(e->d_evtable);
+  cudaFree(e->d_tally_of);
+  cudaFree(e->d_seg);
   cudaFree(e->d_qa);
   cudaFree(e->d_qb);
   cudaFree(e->d_tally);
@@ -929,6 +951,27 @@ int optx_engine_destroy(optx_engine* e) {
   delete e;
   return OPTX_OK;
 }
+
+}  // extern "C"
+
+// Uploads the record table and offsets of the current batch and builds the
+// photon -> record table at the finest resolution the table holds.
+static int engine_upload_records(optx_engine* e, cudaStream_t st) {
+  const uint32_t n = e->n_events;
+  OPTX_CUDA(cudaMemcpyAsync(e->d_params, e->h_params.data(), sizeof(DevParams) * n,
+                            cudaMemcpyHostToDevice, st));
+  OPTX_CUDA(cudaMemcpyAsync(e->d_offsets, e->h_offsets.data(), 8ull * (n + 1ull),
+                            cudaMemcpyHostToDevice, st));
+  uint32_t shift = 0;
+  while (shift < kEvShift && (e->total >> shift) + 2ull > e->ev_entries) ++shift;
+  e->ev_shift = shift;
+  if ((n > 1 || e->gensteps) && e->total > 0)
+    OPTX_CUDA(DISPATCH(e->cfg.math, launch_event_table, e->d_offsets, n, e->d_evtable, e->total,
+                       shift, st));
+  return OPTX_OK;
+}
+
+extern "C" {
 
 int optx_engine_set_events(optx_engine* e, const optx_params* events, const optx_faces* faces,
                            const uint64_t* counts, uint32_t n_events, uint64_t first_id,
@@ -952,16 +995,90 @@ int optx_engine_set_events(optx_engine* e, const optx_params* events, const optx
   }
   e->h_offsets[n_events] = total;
   e->n_events = n_events;
+  e->n_tallies = n_events;
+  e->gensteps = false;
+  e->total = total;
+  e->first_id = first_id;
+  e->P0 = e->h_params[0];
+  return engine_upload_records(e, static_cast<cudaStream_t>(stream));
+}
+
+int optx_engine_set_gensteps(optx_engine* e, const optx_params* events, const optx_faces* faces,
+                             uint32_t n_events, const optx_genstep* gensteps, uint32_t n_gensteps,
+                             uint64_t first_id, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "engine must not be NULL");
+  if (n_events == 0 || n_events > e->max_events)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "n_events must be in [1, max_events]");
+  if (n_gensteps == 0 || n_gensteps > e->cfg.max_gensteps)
+    return fail(OPTX_ERR_INVALID_ARGUMENT,
+                "n_gensteps must be in [1, max_gensteps] (set max_gensteps in optx_wave_config)");
+  if (events == nullptr || gensteps == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "events and gensteps must not be NULL");
+  std::vector<DevParams> ev(n_events);
+  for (uint32_t i = 0; i < n_events; ++i) {
+    OPTX_TRY(check_params(&events[i], faces ? &faces[i] : nullptr));
+    ev[i] = make_dev_params(events[i], faces ? &faces[i] : nullptr);
+  }
+  e->h_params.resize(n_gensteps);
+  e->h_offsets.resize(n_gensteps + 1ull);
+  std::vector<float4> seg(2ull * n_gensteps);
+  std::vector<uint32_t> tally_of(n_gensteps);
+  uint64_t total = 0;
+  for (uint32_t g = 0; g < n_gensteps; ++g) {
+    const optx_genstep& gs = gensteps[g];
+    if (gs.event >= n_events) return fail(OPTX_ERR_INVALID_ARGUMENT, "genstep event index out of range");
+    const float v[8] = {gs.x0, gs.y0, gs.z0, gs.t0, gs.x1, gs.y1, gs.z1, gs.t1};
+    for (float f : v)
+      if (!std::isfinite(f)) return fail(OPTX_ERR_INVALID_ARGUMENT, "genstep coordinates and times must be finite");
+    if (gs.t1 < gs.t0) return fail(OPTX_ERR_INVALID_ARGUMENT, "genstep t1 must be >= t0");
+    DevParams d = ev[gs.event];
+    d.source = kSourceSegment;
+    d.src_x = gs.x0;
+    d.src_y = gs.y0;
+    d.src_z = gs.z0;
+    e->h_params[g] = d;
+    seg[2ull * g] = make_float4(gs.x1, gs.y1, gs.z1, gs.t0);
+    seg[2ull * g + 1] = make_float4(gs.t1 - gs.t0, 0.0f, 0.0f, 0.0f);
+    tally_of[g] = gs.event;
+    e->h_offsets[g] = total;
+    total += gs.n_photons;
+    if (total > e->max_photons)
+      return fail(OPTX_ERR_INVALID_ARGUMENT, "gensteps exceed the engine's max_photons");
+  }
+  e->h_offsets[n_gensteps] = total;
+  e->n_events = n_gensteps;
+  e->n_tallies = n_events;
+  e->gensteps = true;
   e->total = total;
   e->first_id = first_id;
   e->P0 = e->h_params[0];
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  OPTX_CUDA(cudaMemcpyAsync(e->d_params, e->h_params.data(), sizeof(DevParams) * n_events,
-                            cudaMemcpyHostToDevice, st));
-  OPTX_CUDA(cudaMemcpyAsync(e->d_offsets, e->h_offsets.data(), 8ull * (n_events + 1ull),
-                            cudaMemcpyHostToDevice, st));
-  if (n_events > 1 && total > 0)
-    OPTX_CUDA(DISPATCH(e->cfg.math, launch_event_table, e->d_offsets, n_events, e->d_evtable, total, st));
+  OPTX_CUDA(cudaMemcpyAsync(e->d_seg, seg.data(), sizeof(float4) * seg.size(), cudaMemcpyHostToDevice, st));
+  OPTX_CUDA(cudaMemcpyAsync(e->d_tally_of, tally_of.data(), 4ull * n_gensteps, cudaMemcpyHostToDevice, st));
+  OPTX_TRY(engine_upload_records(e, st));
+  // The host vectors must outlive the asynchronous copies.
+  OPTX_CUDA(cudaStreamSynchronize(st));
+  return OPTX_OK;
+}
+
+int optx_run_gensteps(optx_engine* e, const optx_params* events, const optx_faces* faces,
+                      uint32_t n_events, const optx_genstep* gensteps, uint32_t n_gensteps,
+                      uint64_t first_id, uint64_t* host_tallies, optx_event_stats* stats,
+                      optx_timing* timing) {
+  if (e == nullptr || host_tallies == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "engine and host_tallies must not be NULL");
+  optx_timing tm{};
+  const auto t0 = std::chrono::steady_clock::now();
+  OPTX_TRY(optx_engine_set_gensteps(e, events, faces, n_events, gensteps, n_gensteps, first_id, nullptr));
+  OPTX_TRY(optx_engine_run_tally(e, nullptr));
+  OPTX_TRY(optx_engine_get_tallies(e, host_tallies, nullptr));
+  tm.total_ms = ms_since(t0);
+  optx_event_stats s{};
+  OPTX_TRY(optx_engine_stats(e, &s, nullptr));
+  tm.kernel_ms = s.kernels_ms;
+  if (stats) *stats = s;
+  if (timing) *timing = tm;
   return OPTX_OK;
 }
 
@@ -986,7 +1103,7 @@ int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_de
   std::lock_guard<std::mutex> lk(g_mu);
   if (e == nullptr || dev_w_bin == nullptr || dev_grad == nullptr)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "engine, dev_w_bin and dev_grad must not be NULL");
-  if (e->n_events != 1)
+  if (e->n_tallies != 1)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "the adjoint runs on a single-configuration batch");
   const DevParams& P = e->h_params[0];
   // theta = (abs_length, scat_length, reflectivity, tau) of the uploaded configuration.
@@ -1024,7 +1141,7 @@ int optx_engine_get_tallies(optx_engine* e, uint64_t* host_out, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   WaveCtrl c{};
   OPTX_TRY(engine_check_ctrl(e, c, st));
-  OPTX_CUDA(cudaMemcpyAsync(host_out, e->d_tally, 8ull * e->tdev.len * e->n_events,
+  OPTX_CUDA(cudaMemcpyAsync(host_out, e->d_tally, 8ull * e->tdev.len * e->n_tallies,
                             cudaMemcpyDeviceToHost, st));
   OPTX_CUDA(cudaStreamSynchronize(st));
   return OPTX_OK;
@@ -1216,6 +1333,8 @@ extern "C" int optx_wavefront_tally_noalloc(const optx_params* p, const optx_fac
   WaveArgs a;
   std::memset(&a, 0, sizeof(a));
   a.n_events = 1;
+  a.n_tallies = 1;
+  a.ev_shift = kEvShift;
   a.threshold = 28;
   a.cadence = 0;
   a.qcap = kNoAllocQueuePhotons;

@@ -146,22 +146,25 @@ __global__ void history_tally_kernel(const DevParams P, const TallyDev tc, uint6
 // ---------------------------------------------------------------------------
 // Wavefront engine.
 
-// Event of relative photon g: the table gives the event holding photon
-// (g >> kEvShift) << kEvShift; the scan moves past events that end before g
-// (one or two steps when events hold at least 128 photons).
-__device__ __forceinline__ uint32_t find_event(const WaveArgs* __restrict__ A, unsigned long long g) {
-  uint32_t e = __ldg(A->ev_table + (g >> kEvShift));
+// Event (record) of relative photon g: the table gives the record holding photon
+// (g >> shift) << shift; the scan moves past records that end before g (one or
+// two steps when records hold at least 2^shift photons; the host picks the
+// finest shift its table allocation allows).
+__device__ __forceinline__ uint32_t find_event(const WaveArgs* __restrict__ A, unsigned long long g,
+                                               uint32_t shift) {
+  uint32_t e = __ldg(A->ev_table + (g >> shift));
   const unsigned long long* __restrict__ off = A->offsets;
   while (e + 1u < A->n_events && __ldg(off + e + 1u) <= g) ++e;
   return e;
 }
 
-// table[k] = the event that holds photon k << kEvShift: the largest e with
-// offsets[e] <= k << kEvShift, which is never an empty event (one thread per entry).
+// table[k] = the record that holds photon k << shift: the largest e with
+// offsets[e] <= k << shift, which is never an empty record (one thread per entry).
 __global__ void event_table_kernel(const unsigned long long* __restrict__ offsets, uint32_t n_events,
-                                   uint32_t* __restrict__ table, unsigned long long total) {
+                                   uint32_t* __restrict__ table, unsigned long long total,
+                                   uint32_t shift) {
   const unsigned long long k = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const unsigned long long g = k << kEvShift;
+  const unsigned long long g = k << shift;
   if (g >= total) return;
   uint32_t lo = 0, hi = n_events;
   while (hi - lo > 1u) {
@@ -199,7 +202,7 @@ __global__ void wave_prep_kernel(const WaveArgs* __restrict__ A, WaveCtrl* __res
   }
   if (blockIdx.x == 0 && threadIdx.x < 4u && A->grad != nullptr) A->grad[threadIdx.x] = 0.0;
   if (A->tally != nullptr) {
-    const size_t total = static_cast<size_t>(A->n_events) * A->tc.len;
+    const size_t total = static_cast<size_t>(A->n_tallies) * A->tc.len;
     for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
          i += static_cast<size_t>(gridDim.x) * blockDim.x)
       A->tally[i] = 0ull;
@@ -242,7 +245,8 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
     const float4* qin;
     float4* qout;
     unsigned long long fresh_next, first_id, iter_cap;
-    uint32_t n_in, items, T, cadence, qcap, chunk;
+    uint32_t n_in, items, T, cadence, qcap, chunk, ev_shift;
+    const uint32_t* tally_of;
     TallyDev tc;
   };
   __shared__ WaveShared ws;
@@ -259,6 +263,8 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
     ws.first_id = A->first_id;
     ws.iter_cap = A->iter_cap;
     ws.chunk = A->chunk < 32u ? 32u : A->chunk;
+    ws.tally_of = A->tally_of;
+    ws.ev_shift = A->ev_shift;
     ws.tc = A->tc;
   }
   __syncthreads();
@@ -271,6 +277,11 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
   const unsigned long long& first_id = ws.first_id;
   const unsigned long long& iter_cap = ws.iter_cap;
   const uint32_t& wchunk = ws.chunk;
+  // Tally slice of a record (gensteps of one event share a slice).
+  auto slice_of = [&](uint32_t rec) -> uint32_t {
+    const uint32_t* m = ws.tally_of;
+    return m == nullptr ? rec : __ldg(m + rec);
+  };
   const TallyDev& tc = ws.tc;
   const uint32_t n_bins = tc.len - 7u;
   const bool slot_bins = n_bins <= kSlotBins;
@@ -344,8 +355,9 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
     } else if (MODE == kModeTally && BATCH) {
       // Shared-memory atomics into the event's slot when the warp caches it,
       // else global atomics into the event's slice.
-      const int slot = ev == tag0 ? 0 : (ev == tag1 ? 1 : -1);
-      unsigned long long* G = A->tally + static_cast<size_t>(ev) * tc.len;
+      const uint32_t te = slice_of(ev);
+      const int slot = te == tag0 ? 0 : (te == tag1 ? 1 : -1);
+      unsigned long long* G = A->tally + static_cast<size_t>(te) * tc.len;
       if (slot >= 0) {
         unsigned long long* C = s_evc + slot * 8;
         atomicAdd(&C[fate], 1ull);
@@ -488,10 +500,11 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
           } else {
             const unsigned long long g = fresh_next + (item - n_in);
             npidx = static_cast<uint32_t>(g);
-            if (BATCH) nev = find_event(A, g);
+            if (BATCH) nev = find_event(A, g, ws.ev_shift);
             const DevParams& P = params_of<BATCH>(P0, A, nev);
             nr.init(first_id + g, P.key_lo, P.key_hi, 0u);
-            start_photon<MODE == kModeAdjoint>(P, ns, nr, first_id + g, na_aux);
+            const float4* sg = A->seg == nullptr ? nullptr : A->seg + 2u * nev;
+            start_photon<MODE == kModeAdjoint>(P, ns, nr, first_id + g, na_aux, sg);
           }
           float4* e = pantry + (pc + lane) * 7u;
           e[0] = make_float4(ns.px, ns.py, ns.pz, ns.t);
@@ -511,8 +524,8 @@ __global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
         if (kSlots && got > 0u) {
           // Cache the newest event in a slot; keep the slot of the oldest event
           // of this refill if it has one, else replace the slots in turn.
-          const uint32_t e_first = __shfl_sync(kFull, nev, 0);
-          const uint32_t e_last = __shfl_sync(kFull, nev, got - 1u);
+          const uint32_t e_first = slice_of(__shfl_sync(kFull, nev, 0));
+          const uint32_t e_last = slice_of(__shfl_sync(kFull, nev, got - 1u));
           if (e_last != tag0 && e_last != tag1) {
             const uint32_t v = tag0 == e_first ? 1u : (tag1 == e_first ? 0u : victim);
             victim = v ^ 1u;
@@ -755,10 +768,11 @@ cudaError_t launch_wave(int mode, bool batch, int minb, const DevParams& P, cons
 }
 
 cudaError_t launch_event_table(const unsigned long long* offsets, uint32_t n_events,
-                               uint32_t* table, unsigned long long total, cudaStream_t st) {
-  const unsigned long long entries = ((total + (1ull << kEvShift) - 1ull) >> kEvShift);
+                               uint32_t* table, unsigned long long total, uint32_t shift,
+                               cudaStream_t st) {
+  const unsigned long long entries = ((total + (1ull << shift) - 1ull) >> shift);
   event_table_kernel<<<static_cast<unsigned>((entries + 255) / 256), 256, 0, st>>>(offsets, n_events,
-                                                                                 table, total);
+                                                                                 table, total, shift);
   return cudaGetLastError();
 }
 

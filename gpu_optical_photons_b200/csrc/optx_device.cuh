@@ -47,7 +47,7 @@ struct __align__(16) DevParams {
   float src_z;
   uint32_t surf_bits;                      // 2 bits per face 0..4: Polished/Black/Specular/Lambertian
   uint32_t max_steps;
-  uint32_t source;                         // 0 point, 1 uniform in the volume
+  uint32_t source;                         // 0 point, 1 uniform in the volume, 2 genstep segment
   float refl0, refl1, refl2, refl3;        // reflectivity of faces 0..4
   float refl4, eta2_det, eta2_out;         // (n_scint/n_det)^2, (n_scint/n_out)^2 (fresnel.hpp:32-33)
   uint32_t key_lo;
@@ -270,21 +270,39 @@ __device__ __forceinline__ float fresnel_R(float n1, float n2, float eta2, float
 
 // Emission (transport.hpp:55-67): position (3 draws, volume source only),
 // isotropic direction (2), exponential emission time (1).
+//
+// Genstep segments (source 2, an extension with no reference counterpart): the
+// photon starts at src + u1 (end - src) on the segment from src to end and at
+// time t0 + u2 dt + the exponential decay time; u3 is drawn and unused, so the
+// photon consumes the same six words as the reference's sources. `seg` holds
+// (end x, y, z, t0) and (dt, -, -, -) of the photon's genstep (null otherwise).
+constexpr uint32_t kSourceSegment = 2u;
+
 template <bool AUX>
 __device__ __forceinline__ void start_photon(const DevParams& P, Photon& s, Rng& r, uint64_t id,
-                                             ScoreAux& aux) {
+                                             ScoreAux& aux, const float4* seg = nullptr) {
   uint32_t k;
+  float t_start = 0.0f;
   if (P.source == 0u) {
     s.px = P.src_x;
     s.py = P.src_y;
     s.pz = P.src_z;
     k = 3u;
-  } else {
+  } else if (P.source == 1u) {
     const float u1 = r.uniform<0>(), u2 = r.uniform<1>(), u3 = r.uniform<2>();
     s.px = P.hx * (2.0f * u1 - 1.0f);
     s.py = P.hy * (2.0f * u2 - 1.0f);
     s.pz = P.hz * (2.0f * u3 - 1.0f);
     r.o += 3u;  // o stays <= 3: the window still holds the next 5 words
+    k = 3u;
+  } else {
+    const float4 e = seg[0], w = seg[1];
+    const float u1 = r.uniform<0>(), u2 = r.uniform<1>();
+    s.px = P.src_x + u1 * (e.x - P.src_x);
+    s.py = P.src_y + u1 * (e.y - P.src_y);
+    s.pz = P.src_z + u1 * (e.z - P.src_z);
+    t_start = e.w + u2 * w.x;
+    r.o += 3u;
     k = 3u;
   }
   const float ua = r.uniform<0>(), ub = r.uniform<1>(), ue = r.uniform<2>();
@@ -297,6 +315,7 @@ __device__ __forceinline__ void start_photon(const DevParams& P, Photon& s, Rng&
   s.dz = ct;
   s.t = P.tau > 0.0f ? -P.tau * m_log(ue) : 0.0f;
   if (AUX) aux.t_emit = s.t;
+  if (P.source == kSourceSegment) s.t = t_start + s.t;
   s.path = 0.0f;
   s.nb = 0u;
   s.ns = 0u;

@@ -24,7 +24,8 @@ struct TallyDev {
 struct WaveArgs {
   const DevParams* params;              // event table (1 entry when not batched)
   const unsigned long long* offsets;    // n_events + 1 relative photon offsets (batched)
-  const uint32_t* ev_table;             // event of photon (k << kEvShift), k < total >> kEvShift + 1
+  const uint32_t* ev_table;             // record of photon (k << ev_shift), k <= total >> ev_shift
+  // n_events: records in `params` / `offsets` (events, or gensteps)
   uint32_t n_events;
   uint32_t threshold;                   // refill a warp when fewer lanes than this are alive (1..32)
   uint32_t cadence;                     // steps per photon per wave before a forced spill (0 = none)
@@ -48,7 +49,11 @@ struct WaveArgs {
   uint32_t use_graph;                   // 1: the wave loop is a graph while node (set its condition)
   uint32_t wave_cap;                    // watchdog: max waves per run
   uint32_t chunk;                       // consecutive work items a warp claims per grab (>= 32)
-  uint32_t pad2;
+  uint32_t n_tallies;                   // tally slices (= n_events unless records map to events)
+  uint32_t ev_shift;                    // ev_table resolution: one entry per 2^ev_shift photons
+  uint32_t pad3;
+  const uint32_t* tally_of;             // record -> tally slice (null: the record's own index)
+  const float4* seg;                    // genstep records: 2 float4 each (end x,y,z,t0), (dt,-,-,-)
 };
 
 // Dynamic state of a wavefront run (device memory).
@@ -68,7 +73,7 @@ struct WaveCtrl {
 };
 
 enum WaveMode : int { kModeTally = 0, kModeRecords = 1, kModeAdjoint = 2 };
-constexpr uint32_t kEvShift = 7;  // event lookup table: one entry per 128 photons
+constexpr uint32_t kEvShift = 7;  // coarsest event-table resolution: one entry per 128 photons
 // Shared memory of one warp's pantry: 32 ready photons x 112 bytes (7 x 16 B;
 // the 112-byte stride makes 8 lanes' 128-bit accesses hit 8 distinct bank groups).
 constexpr uint32_t kPantryBytesPerWarp = 32u * 112u;
@@ -101,7 +106,8 @@ inline __host__ __device__ uint32_t slot_bin_bytes_per_warp(uint32_t n_bins) {
                           const WaveArgs* A_dev, WaveCtrl* ctrl, int grid, int block,            \
                           size_t smem, cudaStream_t st);                                         \
   cudaError_t launch_event_table(const unsigned long long* offsets, uint32_t n_events,           \
-                                 uint32_t* table, unsigned long long total, cudaStream_t st);    \
+                                 uint32_t* table, unsigned long long total, uint32_t shift,      \
+                                 cudaStream_t st);                                               \
   }
 
 OPTX_DECLARE_LAUNCHERS(fast)

@@ -29,11 +29,12 @@ class WaveConfig:
     use_graph: bool = True
     math: str = "fast"
     chunk: int = 0              # consecutive photons a warp claims per grab (0 = 256)
+    max_gensteps: int = 0       # capacity for set_gensteps (0 = no gensteps)
 
     def to_c(self) -> _lib.CWaveConfig:
         return _lib.CWaveConfig(self.block_size, self.blocks_per_sm, self.threshold, self.cadence,
                                 self.wave_quota, 1 if self.use_graph else -1, _lib.MATH[self.math],
-                                self.chunk, 0)
+                                self.chunk, self.max_gensteps)
 
 
 def _events_c(events):
@@ -88,6 +89,33 @@ class WavefrontEngine:
                   cnt.ctypes.data, len(events), first_id, ctypes.c_void_p(stream or 0))
         self.n_events = len(events)
         self.counts = cnt
+
+    def set_gensteps(self, events, gensteps, first_id: int = 0, stream=0):
+        """Uploads gensteps (a GENSTEP_DTYPE array, see gensteps.py) emitting into
+        `events` (their physics and tally slices); tallies() then has one row per event."""
+        from .gensteps import as_gensteps
+        arr, faces = _events_c(events)
+        g = as_gensteps(gensteps)
+        self._keep = (arr, faces, g)
+        _lib.call("optx_engine_set_gensteps", self._h, ctypes.cast(arr, ctypes.c_void_p),
+                  ctypes.cast(faces, ctypes.c_void_p) if faces is not None else None, len(events),
+                  g.ctypes.data, len(g), first_id, ctypes.c_void_p(stream or 0))
+        self.n_events = len(events)
+        self.counts = np.bincount(g["event"], weights=g["n_photons"], minlength=len(events)).astype(np.uint64)
+
+    def run_gensteps(self, events, gensteps, first_id: int = 0):
+        """One-shot host-buffer genstep run: upload, graph launch, D2H per-event tallies."""
+        from .gensteps import as_gensteps
+        arr, faces = _events_c(events)
+        g = as_gensteps(gensteps)
+        out = np.zeros((len(events), self.tally_config.length), np.uint64)
+        st = _lib.CEventStats()
+        tm = _lib.CTiming()
+        _lib.call("optx_run_gensteps", self._h, ctypes.cast(arr, ctypes.c_void_p),
+                  ctypes.cast(faces, ctypes.c_void_p) if faces is not None else None, len(events),
+                  g.ctypes.data, len(g), first_id, out.ctypes.data, ctypes.byref(st), ctypes.byref(tm))
+        self.n_events = len(events)
+        return out, st.as_dict(), tm.as_dict()
 
     def run_tally(self, stream=0):
         _lib.call("optx_engine_run_tally", self._h, ctypes.c_void_p(stream or 0))

@@ -105,8 +105,24 @@ typedef struct optx_wave_config {
   int32_t math;          /* OPTX_MATH_FAST / OPTX_MATH_EXACT / OPTX_MATH_APPROX */
   uint32_t chunk;        /* consecutive photons a warp claims per grab, 32..2^20 (default 256);
                             results do not depend on it */
-  uint32_t reserved;     /* must be 0 */
+  uint32_t max_gensteps; /* capacity for optx_engine_set_gensteps, 0 = none (default) */
 } optx_wave_config;
+
+/* Extension (no reference counterpart; the reference lists generation on the GPU
+ * from gensteps as future work, README.md section 9 item 7): a genstep, the
+ * compact description of the photons one charged-particle step emits. Its
+ * photons start uniformly on the segment (x0,y0,z0)-(x1,y1,z1), at a time
+ * uniform in [t0, t1] plus the event's exponential decay time (tau), with
+ * isotropic directions; they consume the same six emission draws as the
+ * reference's sources (position fraction, time fraction, one unused word,
+ * direction cos theta, azimuth, decay), then transport with the physics of
+ * their event and add to that event's tally. */
+typedef struct optx_genstep {
+  float x0, y0, z0, t0;  /* segment start (mm), emission window start (ns) */
+  float x1, y1, z1, t1;  /* segment end (mm), emission window end (ns), t1 >= t0 */
+  uint32_t n_photons;    /* photons emitted along this step */
+  uint32_t event;        /* index into the events array: physics and tally slice */
+} optx_genstep;
 
 /* ---- device ---------------------------------------------------------- */
 int optx_abi_version(void);
@@ -172,6 +188,15 @@ int optx_engine_destroy(optx_engine* e);
 int optx_engine_set_events(optx_engine* e, const optx_params* events, const optx_faces* faces,
                            const uint64_t* counts, uint32_t n_events, uint64_t first_id,
                            void* stream);
+/* Uploads a batch of gensteps (extension, see optx_genstep): n_events events
+ * (physics; each event's source fields are ignored) and n_gensteps <= the
+ * engine's max_gensteps gensteps in any order of events. The photons of genstep
+ * g have the Philox ids first_id + (photons of gensteps 0..g-1) + 0, 1, ...; a
+ * run expands them on the device and adds them to per-event tallies (n_events
+ * slices). Blocks until the upload is done. */
+int optx_engine_set_gensteps(optx_engine* e, const optx_params* events, const optx_faces* faces,
+                             uint32_t n_events, const optx_genstep* gensteps, uint32_t n_gensteps,
+                             uint64_t first_id, void* stream);
 /* Runs the uploaded batch; per-event tallies stay on the device (overwritten).
  * Asynchronous on `stream`. */
 int optx_engine_run_tally(optx_engine* e, void* stream);
@@ -203,6 +228,13 @@ int optx_engine_stats(optx_engine* e, optx_event_stats* stats, void* stream);
 int optx_run_batch(optx_engine* e, const optx_params* events, const optx_faces* faces,
                    const uint64_t* counts, uint32_t n_events, uint64_t first_id,
                    uint64_t* host_tallies, optx_event_stats* stats, optx_timing* timing);
+
+/* One-shot genstep run with host buffers (extension): set_gensteps, one graph
+ * launch, D2H of the per-event tallies (host_tallies: n_events x tally length). */
+int optx_run_gensteps(optx_engine* e, const optx_params* events, const optx_faces* faces,
+                      uint32_t n_events, const optx_genstep* gensteps, uint32_t n_gensteps,
+                      uint64_t first_id, uint64_t* host_tallies, optx_event_stats* stats,
+                      optx_timing* timing);
 
 /* ---- wavefront tally without device allocation -------------------------- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc

@@ -387,21 +387,40 @@ inline Surf make_surf(const Params& p, const Faces* f) {
   return s;
 }
 
+// A genstep (the package's extension, no reference counterpart): photons start
+// uniformly on the segment (x0,y0,z0)-(x1,y1,z1) at time t0 + u (t1 - t0) plus the
+// exponential decay time; same 40-byte layout as optx_genstep of include/optx.h.
+struct Genstep {
+  float x0, y0, z0, t0, x1, y1, z1, t1;
+  uint32_t n_photons, event;
+};
+
+// Emission (transport.hpp:55-67). source 2 = genstep segment `g` (extension): the
+// three position words become the segment fraction, the time fraction and an
+// unused word, so the photon draws the same six words as the reference's sources.
 template <class R, class M>
-inline State<R> start_photon(const Params& p, Stream& rng, Extra& ex) {
+inline State<R> start_photon(const Params& p, Stream& rng, Extra& ex, const Genstep* g = nullptr) {
   V3<R> pos;
+  R t_start = R(0.0f);
   if (p.source == 0) {
     pos = {R(p.src_x), R(p.src_y), R(p.src_z)};
-  } else {
+  } else if (p.source == 1) {
     const R u1 = rng.uniform(), u2 = rng.uniform(), u3 = rng.uniform();
     pos = {R(p.hx) * (R(2.0f) * u1 - R(1.0f)), R(p.hy) * (R(2.0f) * u2 - R(1.0f)),
            R(p.hz) * (R(2.0f) * u3 - R(1.0f))};
+  } else {
+    const R u1 = rng.uniform(), u2 = rng.uniform();
+    (void)rng.uniform();
+    pos = {R(g->x0) + u1 * (R(g->x1) - R(g->x0)), R(g->y0) + u1 * (R(g->y1) - R(g->y0)),
+           R(g->z0) + u1 * (R(g->z1) - R(g->z0))};
+    t_start = R(g->t0) + u2 * R(g->t1 - g->t0);  // dt in float, as the engine uploads it
   }
   const R ua = rng.uniform(), ub = rng.uniform();
   const V3<R> dir = sample_isotropic<R, M>(ua, ub);
   const R ue = rng.uniform();
-  const R t = R(p.tau) > R(0.0f) ? -R(p.tau) * Math<R, M>::log(ue) : R(0.0f);
+  R t = R(p.tau) > R(0.0f) ? -R(p.tau) * Math<R, M>::log(ue) : R(0.0f);
   ex.t_emit = fval(t);
+  if (p.source == 2) t = t_start + t;
   return {pos, dir, t, R(0.0f), 0u, 0u};
 }
 
@@ -494,10 +513,10 @@ struct Result {
 };
 
 template <class R, class M>
-inline Result transport(const Params& p, const Surf& sf, uint64_t id) {
+inline Result transport(const Params& p, const Surf& sf, uint64_t id, const Genstep* g = nullptr) {
   Stream rng(p.seed, id);
   Extra ex;
-  State<R> s = start_photon<R, M>(p, rng, ex);
+  State<R> s = start_photon<R, M>(p, rng, ex, g);
   uint8_t fate = MaxSteps;
   int kind = 0;
   for (uint32_t step = 0; step < p.max_steps; ++step) {
@@ -539,11 +558,12 @@ Result transport_dispatch(const Params& p, const Surf& sf, uint64_t id) {
   return transport<R, M>(p, sf, id);
 }
 
-inline Result run_one(int mode, const Params& p, const Surf& sf, uint64_t id) {
+inline Result run_one(int mode, const Params& p, const Surf& sf, uint64_t id,
+                      const Genstep* g = nullptr) {
   switch (mode) {
-    case 1: return transport<float, PortableMath>(p, sf, id);
-    case 2: return transport<double, PlatformMath>(p, sf, id);
-    default: return transport<float, PlatformMath>(p, sf, id);
+    case 1: return transport<float, PortableMath>(p, sf, id, g);
+    case 2: return transport<double, PlatformMath>(p, sf, id, g);
+    default: return transport<float, PlatformMath>(p, sf, id, g);
   }
 }
 
@@ -630,6 +650,54 @@ int oracle_batch_tally(const Params* ev, const uint64_t* offsets, uint32_t n_eve
   for (uint32_t e = 0; e < n_events; ++e) {
     oracle_tally(&ev[e], nullptr, c, offsets[e + 1] - offsets[e], offsets[e], mode, threads,
                  out + static_cast<uint64_t>(e) * L);
+  }
+  return 0;
+}
+
+// Gensteps (extension): genstep g of n_gs emits photons with ids first_id +
+// (photons of gensteps 0..g-1) + k, with the physics of ev[g.event] (surfaces
+// from faces[g.event] when faces is not null) and adds them to that event's
+// tally (out: n_events x tally_len, accumulated into). Records (any pointer may
+// be null) are written in photon order when fate is not null.
+int oracle_genstep_run(const Params* ev, const Faces* faces, uint32_t n_events, const Genstep* gs,
+                       uint64_t n_gs, uint64_t first_id, const TallyConfig* c, int mode, int threads,
+                       uint64_t* out, uint8_t* fate, uint32_t* nb, uint32_t* ns, float* t, float* x,
+                       float* y, float* z, float* path) {
+  const uint64_t L = c ? tally_len(*c) : 0;
+  uint64_t off = 0;
+  for (uint64_t g = 0; g < n_gs; ++g) {
+    const Genstep& G = gs[g];
+    if (G.event >= n_events) return 1;
+    Params p = ev[G.event];
+    p.source = 2;
+    const Surf sf = make_surf(p, faces ? &faces[G.event] : nullptr);
+    const int64_t count = static_cast<int64_t>(G.n_photons);
+    const uint64_t base = off;
+#pragma omp parallel num_threads(threads > 0 ? threads : omp_get_max_threads())
+    {
+      std::vector<uint64_t> local(L, 0);
+#pragma omp for schedule(dynamic, 1024) nowait
+      for (int64_t i = 0; i < count; ++i) {
+        const uint64_t k = base + static_cast<uint64_t>(i);
+        const Result r = run_one(mode, p, sf, first_id + k, &G);
+        if (out) tally_add(local.data(), r, p, *c);
+        if (fate) {
+          fate[k] = r.fate;
+          nb[k] = r.nb;
+          ns[k] = r.ns;
+          t[k] = r.t;
+          x[k] = r.x;
+          y[k] = r.y;
+          z[k] = r.z;
+          path[k] = r.path;
+        }
+      }
+      if (out) {
+#pragma omp critical
+        for (uint64_t q = 0; q < L; ++q) out[static_cast<uint64_t>(G.event) * L + q] += local[q];
+      }
+    }
+    off += G.n_photons;
   }
   return 0;
 }

@@ -48,6 +48,8 @@ def lib():
         L.oracle_records.argtypes = [_P, _P, _u64, _u64, ctypes.c_int, ctypes.c_int] + [_P] * 9
         L.oracle_tally.argtypes = [_P, _P, _P, _u64, _u64, ctypes.c_int, ctypes.c_int, _P]
         L.oracle_batch_tally.argtypes = [_P, _P, ctypes.c_uint32, _P, ctypes.c_int, ctypes.c_int, _P]
+        L.oracle_genstep_run.argtypes = [_P, _P, ctypes.c_uint32, _P, _u64, _u64, _P, ctypes.c_int,
+                                         ctypes.c_int, _P] + [_P] * 8
         L.oracle_adjoint.argtypes = [_P, _P, _u64, _u64, ctypes.c_int, ctypes.c_int, _P,
                                      ctypes.c_double, _P, _P, _P]
         L.oracle_opcount.argtypes = [_P, _P, _u64, _u64, _P]
@@ -159,6 +161,30 @@ def batch_tally(events_c, offsets: np.ndarray, c, mode: int = PLATFORM, threads:
     lib().oracle_batch_tally(ctypes.cast(events_c, ctypes.c_void_p), _ptr(offs), ne,
                              ctypes.byref(cc), mode, threads, _ptr(out))
     return out
+
+
+def genstep_run(events, gensteps, c=None, first_id: int = 0, mode: int = PLATFORM, threads: int = 0,
+                records: bool = False):
+    """Gensteps (the package's extension): per-event tallies (n_events x len, when
+    c is given) and, with records=True, the records of all photons in photon order."""
+    from gpu_optical_photons_b200.gensteps import as_gensteps, photons_of
+    from gpu_optical_photons_b200.wavefront import _events_c
+    arr, faces = _events_c(events)
+    g = as_gensteps(gensteps)
+    out = None
+    cc = None
+    if c is not None:
+        out = np.zeros((len(events), c.length), np.uint64)
+        cc = c.to_c()
+    rec = Records.empty(photons_of(g)) if records else None
+    ptrs = [_ptr(rec[k]) for k in Records.FIELDS] if records else [None] * 8
+    rc = lib().oracle_genstep_run(ctypes.cast(arr, ctypes.c_void_p),
+                                  ctypes.cast(faces, ctypes.c_void_p) if faces is not None else None,
+                                  len(events), _ptr(g), len(g), first_id,
+                                  ctypes.byref(cc) if cc is not None else None, mode, threads,
+                                  _ptr(out), *ptrs)
+    assert rc == 0
+    return out, rec
 
 
 def adjoint(p, c, n: int, w_bin=None, w_det: float = 0.0, first_id: int = 0,

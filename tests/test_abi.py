@@ -58,6 +58,7 @@ def test_struct_layouts():
     assert ctypes.sizeof(_lib.CTiming) == 40
     assert ctypes.sizeof(_lib.CEventStats) == 40
     assert ctypes.sizeof(_lib.CWaveConfig) == 40
+    assert ctypes.sizeof(_lib.CGenstep) == 40
 
 
 def test_invalid_arguments_raise_value_error(lib):
