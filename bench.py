@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--math", default="fast", choices=["fast", "exact", "approx"],
                     help="math mode of the kernels (see include/optx.h)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-history-baseline", action="store_true",
+                    help="skip the plain history-kernel baseline (one launch per event)")
     ap.add_argument("--events", type=int, default=4096)
     ap.add_argument("--host-loop", action="store_true",
                     help="launch the waves from the host instead of the graph while loop "
@@ -171,6 +173,38 @@ def cpu_reference_leg(events, counts, tc, max_events: int, threads: int = 0, fir
     return {"value": steps / dt, "unit": UNIT, "cores": int(cores), "kind": kind,
             "sample": f"events {first}..{max_events - 1} of {len(counts)} ({photons} photons, {steps} photon-steps), "
                       f"run_cpu_tally per event, {dt:.1f} s"}, steps / dt
+
+
+def history_baseline(g, events, counts, tc, first_id: int, math: str, stream, reps: int = 2):
+    """The batch as the plain history kernel runs it: one optx_tally_device launch
+    per event, back to back on one stream (the reference's way to process many
+    events: one run_gpu_tally each), timed with CUDA events after one warm-up
+    pass. Returns (photon-steps/s, ms per pass, tallies of the last pass)."""
+    import torch
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    dev = torch.zeros((len(events), tc.length), dtype=torch.int64, device="cuda")
+    sptr = stream.cuda_stream
+
+    def one_pass():
+        dev.zero_()
+        for i, e in enumerate(events):
+            if counts[i]:
+                g.tally_device(e, tc, int(counts[i]), first_id=first_id + int(offs[i]), out=dev[i],
+                               math=math, stream=sptr)
+
+    one_pass()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        one_pass()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    t = dev.cpu().numpy().astype(np.uint64)
+    m = float(np.median(ms))
+    return steps_of_tallies(t) / (m * 1e-3), m, t
 
 
 def run_reference(args):
@@ -349,6 +383,15 @@ def run_optx(args):
         "clocks": clocks,
         "wall_s_timed": wall,
     }
+    if not args.no_history_baseline:
+        hv, hms, ht = history_baseline(g, events, counts, tc, first_id, args.math, stream)
+        # Same per-photon arithmetic, integer tallies: the two engines agree exactly.
+        assert np.array_equal(ht, tallies), "history and wavefront tallies differ"
+        line["history_baseline"] = {
+            "value": world * hv, "unit": UNIT, "ms_per_step": hms, "launches": len(events),
+            "what": "one history-kernel launch (optx_tally_device) per event, back to back on one "
+                    "stream; identical tallies checked",
+            "speedup_of_value": value / (world * hv)}
     if rank == 0 and not args.no_cpu_baseline:
         base, _ = cpu_reference_leg(events, counts, tc, max_events=min(1024, len(events)))
         line["cpu_baseline"] = base
