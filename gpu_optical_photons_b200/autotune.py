@@ -3,8 +3,9 @@
 Chooses, for a given workload (a batch of events with their photon counts and
 a tally configuration), the engine settings by measurement on the device:
 
-* ``blocks_per_sm`` — resident 256-thread blocks per SM, i.e. the register
-  budget of the wave kernel (2, 3 or 4 blocks: <= 128 / 80 / 64 registers);
+* ``blocks_per_sm`` — the register budget of the wave kernel as resident blocks
+  per SM (2, 3 or 4 blocks of 256 threads: <= 128 / 80 / 64 registers; 7 blocks
+  of 128 threads: <= 72 registers);
 * ``threshold`` — refill a warp when fewer than this many lanes are alive (the
   compaction threshold: higher keeps warps fuller, lower refills less often);
 * ``block_size`` — threads per block;
@@ -58,7 +59,7 @@ def time_config(cfg: WaveConfig, events, counts, tally: TallyConfig, repeats: in
 
 
 def tune(events, counts, tally: TallyConfig, base: WaveConfig | None = None, repeats: int = 3,
-         bps=(2, 3, 4), thresholds=(16, 20, 24, 28, 32), blocks=(128, 256), cadences=(0, 32),
+         bps=(2, 3, 4, 7), thresholds=(16, 20, 24, 28, 32), blocks=(128, 256), cadences=(0, 32),
          quota_fracs=(0.0, 0.25), chunks=(64, 256, 1024), verbose: bool = False):
     """Returns (best WaveConfig, list of measurement dicts)."""
     base = base or WaveConfig()
@@ -88,7 +89,7 @@ def tune(events, counts, tally: TallyConfig, base: WaveConfig | None = None, rep
         if ms < best_ms:
             best_cfg, best_ms = cfg, ms
     for bs in blocks:
-        if bs == best_cfg.block_size:
+        if bs == best_cfg.block_size or best_cfg.blocks_per_sm == 7:  # 7 implies 128-thread blocks
             continue
         cfg = replace(best_cfg, block_size=bs)  # same register budget, smaller blocks
         ms = measure(cfg)

@@ -33,6 +33,9 @@ def main(argv=None):
     ap.add_argument("--block", type=int, default=256)
     ap.add_argument("--threshold", type=int, default=24)
     ap.add_argument("--cadence", type=int, default=0)
+    ap.add_argument("--bps", type=int, default=0, help="wave engine register budget: 2/3/4 (blocks of "
+                    "256) or 7 (blocks of 128); 0 = default")
+    ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--host-loop", action="store_true", help="launch waves from the host (no graph)")
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--out", help="write records / tally .npy files and meta.json here "
@@ -99,7 +102,7 @@ def main(argv=None):
                 io.write_records(a.out, r, meta)
     else:
         cfg = WaveConfig(block_size=a.block, threshold=a.threshold, cadence=a.cadence,
-                         use_graph=not a.host_loop, math=a.math)
+                         blocks_per_sm=a.bps, chunk=a.chunk, use_graph=not a.host_loop, math=a.math)
         eng = WavefrontEngine(c, 1, n, cfg)
         eng.set_events([p], [n])
         for _ in range(a.repeat):

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -37,10 +38,13 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+// On failure the thread's last CUDA error is read back (cleared), so that a
+// non-sticky error is not reported again by a later, unrelated launch.
 #define OPTX_CUDA(call)                                                                   \
   do {                                                                                    \
     const cudaError_t err_ = (call);                                                      \
     if (err_ != cudaSuccess) {                                                            \
+      (void)cudaGetLastError();                                                           \
       return fail(OPTX_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(err_) + \
                                      " at " __FILE__ ":" + std::to_string(__LINE__) +     \
                                      " (" #call ")");                                     \
@@ -317,9 +321,11 @@ size_t wave_smem(const optx_engine* e, int mode, bool batch) {
   return pantry;
 }
 
-// Register-budget variant of the wave kernel: 2, 3 or 4 blocks of 256 threads per SM.
+// Register-budget variant of the wave kernel: 2, 3 or 4 blocks of 256 threads
+// per SM, or 7 blocks of 128 threads.
 int engine_minb(const optx_engine* e) {
-  const int b = e->cfg.blocks_per_sm > 0 ? e->cfg.blocks_per_sm : 4;
+  const int b = e->cfg.blocks_per_sm > 0 ? e->cfg.blocks_per_sm : 3;
+  if (b == 7) return 7;
   return std::max(2, std::min(4, b));
 }
 
@@ -327,10 +333,17 @@ int engine_grid(optx_engine* e, int mode, bool batch, int& grid) {
   const size_t smem = wave_smem(e, mode, batch);
   const int math = e->cfg.math;
   const int minb = engine_minb(e);
+  int dev = 0, max_smem = 0;
+  OPTX_CUDA(cudaGetDevice(&dev));
+  OPTX_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (smem > static_cast<size_t>(max_smem))
+    return fail(OPTX_ERR_RUNTIME, "wavefront kernel needs " + std::to_string(smem) +
+                                      " bytes of shared memory per block; reduce xy_bins / time_bins");
   if (smem > 48 * 1024) OPTX_CUDA(DISPATCH(math, wave_set_smem, mode, batch, minb, smem));
   int bps = DISPATCH(math, wave_blocks_per_sm, mode, batch, minb, e->cfg.block_size, smem);
   if (bps <= 0) return fail(OPTX_ERR_RUNTIME, "wavefront kernel cannot be resident with this block size / tally");
-  if (e->cfg.blocks_per_sm > 0) bps = std::min(bps, e->cfg.blocks_per_sm * (256 / e->cfg.block_size));
+  if (e->cfg.blocks_per_sm == 7) bps = std::min(bps, 7);
+  else if (e->cfg.blocks_per_sm > 0) bps = std::min(bps, e->cfg.blocks_per_sm * (256 / e->cfg.block_size));
   grid = bps * e->n_sm;
   return OPTX_OK;
 }
@@ -603,6 +616,71 @@ void parallel_copy(const std::vector<std::tuple<void*, const void*, size_t>>& jo
   for (auto& x : th) x.join();
 }
 
+// ---- engines behind the reference-API host calls ------------------------------
+// optx_run_tally and optx_run_records run the wavefront engine: the same
+// per-photon arithmetic as the history kernels (bit-identical records, equal
+// integer tallies) at 1.4-2x their speed on one configuration. One engine per
+// (device, math mode, tally configuration, photon capacity) is created on first
+// use and kept until optx_release_cache; its mutex serialises a call's upload /
+// run / read-back sequence. Lock order: g_pipe_mu, then an engine's mu, then g_mu
+// (taken inside the optx_engine_* calls).
+struct ApiEngine {
+  int device = -1;
+  int math = 0;
+  optx_tally_config tc{};
+  uint64_t cap = 0;
+  optx_engine* e = nullptr;
+  std::mutex mu;
+};
+std::vector<std::unique_ptr<ApiEngine>> g_api;  // guarded by g_mu
+std::mutex g_pipe_mu;                           // the records pipeline (g_pipe)
+constexpr uint64_t kApiMaxCap = 1ull << 27;     // photons per engine run
+
+// Photon capacity of an engine serving runs of n photons: a power of two in
+// [2^20, 2^27], so that a few engines serve all sizes.
+uint64_t api_capacity(uint64_t n) {
+  uint64_t c = 1ull << 20;
+  while (c < n && c < kApiMaxCap) c <<= 1;
+  return c;
+}
+
+// Finds or creates the engine. OPTX_ERR_RUNTIME means the wave kernel cannot be
+// resident beside these histograms (the caller then runs the history kernel).
+int api_engine(int math, const optx_tally_config& tc, uint64_t cap, ApiEngine** out) {
+  int dev = 0;
+  OPTX_CUDA(cudaGetDevice(&dev));
+  auto match = [&](const ApiEngine& a) {
+    return a.device == dev && a.math == math && a.cap >= cap && a.tc.time_bins == tc.time_bins &&
+           a.tc.time_max == tc.time_max && a.tc.xy_bins == tc.xy_bins;
+  };
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto& a : g_api)
+      if (match(*a)) {
+        *out = a.get();
+        return OPTX_OK;
+      }
+  }
+  optx_wave_config cfg{};
+  cfg.block_size = 128;   // the 72-register budget: 28 warps per SM, the fastest
+  cfg.blocks_per_sm = 7;  // single-configuration variant on the reference setups
+  cfg.threshold = 28;
+  cfg.use_graph = 1;
+  cfg.math = math;
+  optx_engine* e = nullptr;
+  OPTX_TRY(optx_engine_create(&tc, 1, cap, &cfg, &e));
+  auto a = std::make_unique<ApiEngine>();
+  a->device = dev;
+  a->math = math;
+  a->tc = tc;
+  a->cap = cap;
+  a->e = e;
+  std::lock_guard<std::mutex> lk(g_mu);
+  *out = a.get();
+  g_api.push_back(std::move(a));
+  return OPTX_OK;
+}
+
 }  // namespace
 
 // =============================================================================
@@ -635,19 +713,27 @@ int optx_gpu_device_name(char* buf, size_t len) {
 const char* optx_last_error(void) { return g_err.c_str(); }
 
 int optx_release_cache(void) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (g_cache.rec) cudaFree(g_cache.rec);
-  if (g_cache.tally) cudaFree(g_cache.tally);
-  if (g_cache.e0) cudaEventDestroy(g_cache.e0);
-  if (g_cache.e1) cudaEventDestroy(g_cache.e1);
-  g_cache = Cache{};
+  std::vector<std::unique_ptr<ApiEngine>> engines;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_cache.rec) cudaFree(g_cache.rec);
+    if (g_cache.tally) cudaFree(g_cache.tally);
+    if (g_cache.e0) cudaEventDestroy(g_cache.e0);
+    if (g_cache.e1) cudaEventDestroy(g_cache.e1);
+    g_cache = Cache{};
+    engines.swap(g_api);
+  }
+  for (auto& a : engines) {  // wait for calls still using an engine
+    std::lock_guard<std::mutex> lk(a->mu);
+    optx_engine_destroy(a->e);
+  }
   return OPTX_OK;
 }
 
 int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
                                 const optx_records* out, int block_size, uint64_t first_id,
                                 uint64_t chunk, int math, optx_timing* timing) {
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk(g_pipe_mu);
   OPTX_TRY(check_params(p, faces));
   OPTX_TRY(check_block(block_size));
   OPTX_TRY(check_math(math));
@@ -666,6 +752,14 @@ int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
       1, std::min<uint64_t>({n, chunk ? chunk : (uint64_t{1} << 24), uint64_t{1} << 22}));
   const auto ta = std::chrono::steady_clock::now();
   OPTX_TRY(pipe_ensure(cap));
+  // The wavefront engine writes each chunk's records (the history kernel when the
+  // engine cannot be created, which a records run never needs in practice).
+  ApiEngine* ae = nullptr;
+  const optx_tally_config no_tally{1u, 1.0f, 1u};
+  const int erc = api_engine(math, no_tally, api_capacity(cap), &ae);
+  if (erc != OPTX_OK && erc != OPTX_ERR_RUNTIME) return erc;
+  std::unique_lock<std::mutex> elk;
+  if (erc == OPTX_OK) elk = std::unique_lock<std::mutex>(ae->mu);
   tm.alloc_ms = ms_since(ta);
   void* outs[8] = {out->fate, out->n_boundary, out->n_scatter, out->t, out->x, out->y, out->z, out->path};
   bool direct = true;
@@ -700,7 +794,14 @@ int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
                        reinterpret_cast<float*>(dv[3]), reinterpret_cast<float*>(dv[4]),
                        reinterpret_cast<float*>(dv[5]), reinterpret_cast<float*>(dv[6]),
                        reinterpret_cast<float*>(dv[7])};
-    OPTX_CUDA(DISPATCH(math, launch_history_records, P, first_id + done, m, d, block_size, g_pipe.comp));
+    if (ae != nullptr) {
+      const uint64_t cnt = m;
+      const optx_records dr{d.fate, d.n_boundary, d.n_scatter, d.t, d.x, d.y, d.z, d.path};
+      OPTX_TRY(optx_engine_set_events(ae->e, p, faces, &cnt, 1, first_id + done, g_pipe.comp));
+      OPTX_TRY(optx_engine_run_records(ae->e, &dr, g_pipe.comp));
+    } else {
+      OPTX_CUDA(DISPATCH(math, launch_history_records, P, first_id + done, m, d, block_size, g_pipe.comp));
+    }
     OPTX_CUDA(cudaEventRecord(g_pipe.k1[b], g_pipe.comp));
     OPTX_CUDA(cudaStreamWaitEvent(g_pipe.copy, g_pipe.k1[b], 0));
     auto hv = views(b, true);
@@ -739,7 +840,6 @@ int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
 int optx_run_tally(const optx_params* p, const optx_faces* faces, const optx_tally_config* c,
                    uint64_t n, uint64_t* tally_out, int block_size, uint64_t first_id, int math,
                    optx_timing* timing) {
-  std::lock_guard<std::mutex> lk(g_mu);
   OPTX_TRY(check_params(p, faces));
   OPTX_TRY(check_block(block_size));
   OPTX_TRY(check_math(math));
@@ -747,9 +847,40 @@ int optx_run_tally(const optx_params* p, const optx_faces* faces, const optx_tal
   OPTX_TRY(make_tally_dev(c, td));
   if (tally_out == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "tally_out must not be NULL");
   OPTX_TRY(ensure_device());
-  OPTX_TRY(cache_events());
   optx_timing tm{};
   const auto t0 = std::chrono::steady_clock::now();
+  if (n > 0) {
+    // The wavefront engine, in runs of at most its capacity, tallies summed on the host.
+    ApiEngine* ae = nullptr;
+    const int erc = api_engine(math, *c, api_capacity(n), &ae);
+    if (erc != OPTX_OK && erc != OPTX_ERR_RUNTIME) return erc;
+    if (erc == OPTX_OK) {
+      tm.alloc_ms = ms_since(t0);
+      std::lock_guard<std::mutex> elk(ae->mu);
+      std::vector<uint64_t> part(td.len);
+      std::memset(tally_out, 0, td.len * 8ull);
+      for (uint64_t done = 0; done < n;) {
+        const uint64_t m = std::min(ae->cap, n - done);
+        OPTX_TRY(optx_engine_set_events(ae->e, p, faces, &m, 1, first_id + done, nullptr));
+        OPTX_TRY(optx_engine_run_tally(ae->e, nullptr));
+        const auto tc = std::chrono::steady_clock::now();
+        OPTX_TRY(optx_engine_get_tallies(ae->e, part.data(), nullptr));
+        tm.d2h_ms += ms_since(tc);
+        for (uint32_t k = 0; k < td.len; ++k) tally_out[k] += part[k];
+        optx_event_stats s{};
+        OPTX_TRY(optx_engine_stats(ae->e, &s, nullptr));
+        tm.kernel_ms += s.kernels_ms;
+        done += m;
+      }
+      tm.total_ms = ms_since(t0);
+      if (timing) *timing = tm;
+      return OPTX_OK;
+    }
+  }
+  // The history kernel: n = 0, or the wave kernel's pantries do not fit beside
+  // these histograms in shared memory.
+  std::lock_guard<std::mutex> lk(g_mu);
+  OPTX_TRY(cache_events());
   const DevParams P = make_dev_params(*p, faces);
   const size_t smem = static_cast<size_t>(td.len - 7u) * 4u;
   int dev = 0, max_smem = 0;
@@ -860,6 +991,10 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
   if (k.block_size == 0) k.block_size = 256;
   if (k.block_size <= 0 || k.block_size % 32 != 0 || k.block_size > 256)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "wavefront block_size must be a multiple of 32 <= 256");
+  if (k.blocks_per_sm == 7 && k.block_size != 128)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "blocks_per_sm 7 (72-register budget) needs block_size 128");
+  if (k.blocks_per_sm != 0 && k.blocks_per_sm != 7 && (k.blocks_per_sm < 2 || k.blocks_per_sm > 4))
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "blocks_per_sm must be 0 (default), 2, 3, 4 or 7");
   if (k.threshold == 0) k.threshold = 28;
   if (k.threshold > 32) return fail(OPTX_ERR_INVALID_ARGUMENT, "threshold must be 1..32");
   if (k.use_graph == 0) k.use_graph = 1;

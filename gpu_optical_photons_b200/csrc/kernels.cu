@@ -218,10 +218,14 @@ __device__ __forceinline__ const DevParams& params_of(const DevParams& P0,
   return P0;
 }
 
-// MINB: resident blocks of 256 threads per SM the register allocation must allow
-// (2: <= 128 registers, 3: <= 80, 4: <= 64); a tuning knob of the engine.
+// MINB: the register budget, as the resident blocks per SM the allocation must
+// allow: 2, 3 or 4 blocks of 256 threads (<= 128 / 80 / 64 registers), or 7
+// blocks of 128 threads (<= 72 registers, 28 warps per SM); a tuning knob.
+template <int MINB>
+constexpr int wave_max_threads() { return MINB >= 5 ? 128 : 256; }
+
 template <int MODE, bool BATCH, int MINB>
-__global__ void __launch_bounds__(256, MINB) wave_kernel(const DevParams P0,
+__global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(const DevParams P0,
                                                       const WaveArgs* __restrict__ A,
                                                       WaveCtrl* __restrict__ ctrl) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -736,6 +740,7 @@ static const void* kfn(int minb) {
   switch (minb) {
     case 3: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 3>);
     case 4: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 4>);
+    case 7: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 7>);
     default: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 2>);
   }
 }

@@ -22,7 +22,7 @@ from .backend import Tally, _stream_ptr, _crec_from_torch
 @dataclass
 class WaveConfig:
     block_size: int = 256
-    blocks_per_sm: int = 0      # resident 256-thread blocks per SM (2/3/4 = register budget); 0 = 4
+    blocks_per_sm: int = 0      # register budget: 2/3/4 blocks of 256 (128/80/64 regs), 7 blocks of 128 (72); 0 = 3
     threshold: int = 28         # refill when fewer lanes than this are alive
     cadence: int = 0            # forced spill after this many steps per wave (0 = off)
     wave_quota: int = 0         # fresh photons per wave (0 = all)
@@ -32,7 +32,9 @@ class WaveConfig:
     max_gensteps: int = 0       # capacity for set_gensteps (0 = no gensteps)
 
     def to_c(self) -> _lib.CWaveConfig:
-        return _lib.CWaveConfig(self.block_size, self.blocks_per_sm, self.threshold, self.cadence,
+        # the 72-register budget runs 128-thread blocks
+        bs = 128 if self.blocks_per_sm == 7 and self.block_size == 256 else self.block_size
+        return _lib.CWaveConfig(bs, self.blocks_per_sm, self.threshold, self.cadence,
                                 self.wave_quota, 1 if self.use_graph else -1, _lib.MATH[self.math],
                                 self.chunk, self.max_gensteps)
 

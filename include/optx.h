@@ -96,8 +96,10 @@ typedef struct optx_event_stats {
 /* Wavefront engine configuration. Zero fields take defaults. */
 typedef struct optx_wave_config {
   int32_t block_size;    /* threads per block, multiple of 32, <= 256 (default 256) */
-  int32_t blocks_per_sm; /* resident 256-thread blocks per SM: 2, 3 or 4 (register budget
-                            <= 128 / 80 / 64); the persistent grid is that x SMs (default 4) */
+  int32_t blocks_per_sm; /* register budget as resident blocks per SM: 2, 3 or 4 blocks of 256
+                            threads (<= 128 / 80 / 64 registers), or 7 blocks of 128 threads
+                            (<= 72 registers; needs block_size 128); the persistent grid is that
+                            x SMs (default 3) */
   uint32_t threshold;    /* refill a warp when fewer than this many lanes are alive, 1..32 (default 28) */
   uint32_t cadence;      /* steps per photon per wave before a forced spill, 0 = none (default 0) */
   uint64_t wave_quota;   /* fresh photons admitted per wave, 0 = all (default) */

@@ -174,6 +174,16 @@ def test_edge_cases(engine):
         engine.run_gpu_records(p, 10, block_size=100)
     with pytest.raises(engine.OptxError):
         engine.run_gpu_tally(p, P.TallyConfig(100, 50.0, 300), 10)  # 360 KB of shared-memory bins
+    # the failure leaves no CUDA error behind for the next launch
+    rec, _ = engine.run_gpu_records(p, 1000)
+    assert len(rec) == 1000
+    # 223 KB of bins: too many for the wavefront engine beside its pantries, so the
+    # host call runs the history kernel, with the same result as the device call
+    c = P.TallyConfig(100, 50.0, 236)
+    _, flat, _ = engine.run_gpu_tally(p, c, 20_000, first_id=5)
+    dev = engine.tally_device(p, c, 20_000, first_id=5)
+    assert np.array_equal(flat, dev.cpu().numpy().astype(np.uint64))
+    assert flat[:5].sum() == 20_000
 
 
 def test_records_pipeline_pinned_and_pageable(engine):
