@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--math", default="fast", choices=["fast", "exact", "approx"],
                     help="math mode of the kernels (see include/optx.h)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-math", action="store_true",
+                    help="skip timing the same batch in the other two math modes")
     ap.add_argument("--no-history-baseline", action="store_true",
                     help="skip the plain history-kernel baseline (one launch per event)")
     ap.add_argument("--events", type=int, default=4096)
@@ -383,6 +385,36 @@ def run_optx(args):
         "clocks": clocks,
         "wall_s_timed": wall,
     }
+    if not args.no_other_math:
+        # The same batch and engine settings in the other math modes (EXACT: bitwise
+        # parity with the reference CPU build; APPROX: hardware transcendental units).
+        from dataclasses import replace
+        other = {}
+        for m in ("fast", "exact", "approx"):
+            if m == args.math:
+                continue
+            e2 = WavefrontEngine(tc, len(events), n_photons, replace(cfg, math=m))
+            e2.set_events(events, counts, first_id, stream=sptr)
+            for _ in range(args.warmup):
+                e2.run_tally(stream=sptr)
+            torch.cuda.synchronize()
+            ms = []
+            for _ in range(min(args.steps, 20)):
+                flush.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                e2.run_tally(stream=sptr)
+                b.record(stream)
+                torch.cuda.synchronize()
+                ms.append(a.elapsed_time(b))
+            t2 = e2.tallies(stream=sptr)
+            e2.close()
+            mm = float(np.mean(ms))
+            if pg:
+                mm = max_over_ranks(mm, pg, device="cuda")
+            other[m] = {"value": world * steps_of_tallies(t2) / (mm * 1e-3), "ms_per_step": mm,
+                        "photon_steps_per_step": steps_of_tallies(t2)}
+        line["other_math_modes"] = other
     if not args.no_history_baseline:
         hv, hms, ht = history_baseline(g, events, counts, tc, first_id, args.math, stream)
         # Same per-photon arithmetic, integer tallies: the two engines agree exactly.

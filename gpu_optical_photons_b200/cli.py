@@ -26,12 +26,14 @@ CONFIGS = {"default": lambda: (P.SimParams(), P.TallyConfig()),
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--config", default="config1", choices=sorted(CONFIGS))
-    ap.add_argument("--engine", default="history", choices=["history", "wave"])
+    ap.add_argument("--engine", default="history", choices=["history", "wave", "gensteps"],
+                    help="gensteps: --n straight muon tracks through the cube (1 mm gensteps, "
+                         "200 photons/mm) expanded into photons by the wavefront engine")
     ap.add_argument("--mode", default="tally", choices=["tally", "records"])
     ap.add_argument("--n", type=float, default=1e6)
     ap.add_argument("--math", default="fast", choices=["fast", "exact", "approx"])
     ap.add_argument("--block", type=int, default=256)
-    ap.add_argument("--threshold", type=int, default=24)
+    ap.add_argument("--threshold", type=int, default=28)
     ap.add_argument("--cadence", type=int, default=0)
     ap.add_argument("--bps", type=int, default=0, help="wave engine register budget: 2/3/4 (blocks of "
                     "256) or 7 (blocks of 128); 0 = default")
@@ -100,6 +102,29 @@ def main(argv=None):
                 from . import io
                 meta = io.params_to_json(p, io.RunOptions("gpu", "records", n, 1, a.block, c))
                 io.write_records(a.out, r, meta)
+    elif a.engine == "gensteps":
+        from . import gensteps as G
+        events, gs = G.muon_events(n, seed=p.seed)
+        cfg = WaveConfig(block_size=a.block, threshold=a.threshold, cadence=a.cadence,
+                         blocks_per_sm=a.bps, chunk=a.chunk, use_graph=not a.host_loop, math=a.math,
+                         max_gensteps=len(gs))
+        eng = WavefrontEngine(c, len(events), G.photons_of(gs), cfg)
+        eng.set_gensteps(events, gs)
+        for _ in range(a.repeat):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.run_tally()
+            torch.cuda.synchronize()
+            times.append((time.perf_counter() - t0) * 1e3)
+        tl = eng.tallies()
+        out["stats"] = eng.stats()
+        out["gensteps"] = len(gs)
+        out["photons"] = G.photons_of(gs)
+        eng.close()
+        flat = None
+        out["steps"] = int(tl[:, -2].sum() + tl[:, -1].sum() + tl[:, 1].sum())
+        out["fates"] = [int(v) for v in tl[:, :5].sum(0)]
+        n = out["photons"]
     else:
         cfg = WaveConfig(block_size=a.block, threshold=a.threshold, cadence=a.cadence,
                          blocks_per_sm=a.bps, chunk=a.chunk, use_graph=not a.host_loop, math=a.math)
