@@ -278,6 +278,7 @@ struct optx_engine {
   unsigned long long* d_offsets = nullptr;
   uint32_t* d_evtable = nullptr;
   uint32_t* d_tally_of = nullptr;  // genstep -> event (gensteps only)
+  DevParams* d_phys = nullptr;     // physics per event (gensteps only)
   float4* d_seg = nullptr;         // genstep segment ends and time windows
   float4* d_qa = nullptr;
   float4* d_qb = nullptr;
@@ -355,6 +356,7 @@ int engine_upload_args(optx_engine* e, int mode, bool batch, int grid, cudaGraph
   WaveArgs a;
   std::memset(&a, 0, sizeof(a));
   a.params = e->d_params;
+  a.phys = e->gensteps ? e->d_phys : e->d_params;
   a.offsets = e->d_offsets;
   a.ev_table = e->d_evtable;
   a.n_events = e->n_events;
@@ -1051,6 +1053,8 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
        (rc = alloc(reinterpret_cast<void**>(&e->d_tally_of), 4ull * k.max_gensteps))) ||
       (k.max_gensteps > 0 &&
        (rc = alloc(reinterpret_cast<void**>(&e->d_seg), 32ull * k.max_gensteps))) ||
+      (k.max_gensteps > 0 &&
+       (rc = alloc(reinterpret_cast<void**>(&e->d_phys), sizeof(DevParams) * max_events))) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_qa), qcap * 64ull)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_qb), qcap * 64ull)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_tally), 8ull * td.len * max_events)) ||
@@ -1076,6 +1080,7 @@ int optx_engine_destroy(optx_engine* e) {
   cudaFree(e->d_evtable);
   cudaFree(e->d_tally_of);
   cudaFree(e->d_seg);
+  cudaFree(e->d_phys);
   cudaFree(e->d_qa);
   cudaFree(e->d_qb);
   cudaFree(e->d_tally);
@@ -1191,6 +1196,7 @@ int optx_engine_set_gensteps(optx_engine* e, const optx_params* events, const op
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   OPTX_CUDA(cudaMemcpyAsync(e->d_seg, seg.data(), sizeof(float4) * seg.size(), cudaMemcpyHostToDevice, st));
   OPTX_CUDA(cudaMemcpyAsync(e->d_tally_of, tally_of.data(), 4ull * n_gensteps, cudaMemcpyHostToDevice, st));
+  OPTX_CUDA(cudaMemcpyAsync(e->d_phys, ev.data(), sizeof(DevParams) * n_events, cudaMemcpyHostToDevice, st));
   OPTX_TRY(engine_upload_records(e, st));
   // The host vectors must outlive the asynchronous copies.
   OPTX_CUDA(cudaStreamSynchronize(st));

@@ -209,12 +209,13 @@ __global__ void wave_prep_kernel(const WaveArgs* __restrict__ A, WaveCtrl* __res
   }
 }
 
-// Parameters of a lane's photon: the kernel argument (one configuration) or the
+// Physics of a lane's photon: the kernel argument (one configuration) or its
 // event's record in global memory, read field by field where the step uses it.
+// Lanes hold event indices; genstep records are read only at emission.
 template <bool BATCH>
 __device__ __forceinline__ const DevParams& params_of(const DevParams& P0,
                                                       const WaveArgs* __restrict__ A, uint32_t ev) {
-  if (BATCH) return A->params[ev];
+  if (BATCH) return A->phys[ev];
   return P0;
 }
 
@@ -281,8 +282,8 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
   const unsigned long long& first_id = ws.first_id;
   const unsigned long long& iter_cap = ws.iter_cap;
   const uint32_t& wchunk = ws.chunk;
-  // Tally slice of a record (gensteps of one event share a slice).
-  auto slice_of = [&](uint32_t rec) -> uint32_t {
+  // Event of a record (a genstep's event; a plain batch's records are its events).
+  auto event_of = [&](uint32_t rec) -> uint32_t {
     const uint32_t* m = ws.tally_of;
     return m == nullptr ? rec : __ldg(m + rec);
   };
@@ -359,9 +360,8 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     } else if (MODE == kModeTally && BATCH) {
       // Shared-memory atomics into the event's slot when the warp caches it,
       // else global atomics into the event's slice.
-      const uint32_t te = slice_of(ev);
-      const int slot = te == tag0 ? 0 : (te == tag1 ? 1 : -1);
-      unsigned long long* G = A->tally + static_cast<size_t>(te) * tc.len;
+      const int slot = ev == tag0 ? 0 : (ev == tag1 ? 1 : -1);
+      unsigned long long* G = A->tally + static_cast<size_t>(ev) * tc.len;
       if (slot >= 0) {
         unsigned long long* C = s_evc + slot * 8;
         atomicAdd(&C[fate], 1ull);
@@ -505,10 +505,11 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
             const unsigned long long g = fresh_next + (item - n_in);
             npidx = static_cast<uint32_t>(g);
             if (BATCH) nev = find_event(A, g, ws.ev_shift);
-            const DevParams& P = params_of<BATCH>(P0, A, nev);
-            nr.init(first_id + g, P.key_lo, P.key_hi, 0u);
+            const DevParams& R = BATCH ? A->params[nev] : P0;  // the photon's record
+            nr.init(first_id + g, R.key_lo, R.key_hi, 0u);
             const float4* sg = A->seg == nullptr ? nullptr : A->seg + 2u * nev;
-            start_photon<MODE == kModeAdjoint>(P, ns, nr, first_id + g, na_aux, sg);
+            start_photon<MODE == kModeAdjoint>(R, ns, nr, first_id + g, na_aux, sg);
+            if (BATCH) nev = event_of(nev);  // from here on the photon needs only its event
           }
           float4* e = pantry + (pc + lane) * 7u;
           e[0] = make_float4(ns.px, ns.py, ns.pz, ns.t);
@@ -528,8 +529,8 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
         if (kSlots && got > 0u) {
           // Cache the newest event in a slot; keep the slot of the oldest event
           // of this refill if it has one, else replace the slots in turn.
-          const uint32_t e_first = slice_of(__shfl_sync(kFull, nev, 0));
-          const uint32_t e_last = slice_of(__shfl_sync(kFull, nev, got - 1u));
+          const uint32_t e_first = __shfl_sync(kFull, nev, 0);
+          const uint32_t e_last = __shfl_sync(kFull, nev, got - 1u);
           if (e_last != tag0 && e_last != tag1) {
             const uint32_t v = tag0 == e_first ? 1u : (tag1 == e_first ? 0u : victim);
             victim = v ^ 1u;

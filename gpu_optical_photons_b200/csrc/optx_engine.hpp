@@ -22,7 +22,8 @@ struct TallyDev {
 // Wavefront run description, resident in device memory (the host writes it
 // before each run; kernels read it, so a captured graph stays valid).
 struct WaveArgs {
-  const DevParams* params;              // event table (1 entry when not batched)
+  const DevParams* params;              // records: events, or gensteps (1 entry when not batched)
+  const DevParams* phys;                // physics per event (= params unless gensteps)
   const unsigned long long* offsets;    // n_events + 1 relative photon offsets (batched)
   const uint32_t* ev_table;             // record of photon (k << ev_shift), k <= total >> ev_shift
   // n_events: records in `params` / `offsets` (events, or gensteps)
@@ -49,10 +50,10 @@ struct WaveArgs {
   uint32_t use_graph;                   // 1: the wave loop is a graph while node (set its condition)
   uint32_t wave_cap;                    // watchdog: max waves per run
   uint32_t chunk;                       // consecutive work items a warp claims per grab (>= 32)
-  uint32_t n_tallies;                   // tally slices (= n_events unless records map to events)
+  uint32_t n_tallies;                   // events = tally slices (= n_events unless gensteps)
   uint32_t ev_shift;                    // ev_table resolution: one entry per 2^ev_shift photons
   uint32_t pad3;
-  const uint32_t* tally_of;             // record -> tally slice (null: the record's own index)
+  const uint32_t* tally_of;             // record -> event (null: the record's own index)
   const float4* seg;                    // genstep records: 2 float4 each (end x,y,z,t0), (dt,-,-,-)
 };
 
