@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--math", default="fast", choices=["fast", "exact", "approx"],
                     help="math mode of the kernels (see include/optx.h)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint replay / forward cost measurement")
     ap.add_argument("--no-other-math", action="store_true",
                     help="skip timing the same batch in the other two math modes")
     ap.add_argument("--no-history-baseline", action="store_true",
@@ -207,6 +209,38 @@ def history_baseline(g, events, counts, tc, first_id: int, math: str, stream, re
     t = dev.cpu().numpy().astype(np.uint64)
     m = float(np.median(ms))
     return steps_of_tallies(t) / (m * 1e-3), m, t
+
+
+def adjoint_cost(math: str, n: int = 10_000_000, reps: int = 5) -> dict:
+    """Cost of the path-replay adjoint against one forward run on the calibration
+    setup (the Lambertian cube with Rayleigh scattering and a volume source at
+    theta = (La 1000, Ls 700, R 0.95, tau 4), 1e7 photons, 500 arrival-time bins):
+    median CUDA-event times of the forward tally and of the replay that
+    accumulates dLoss/dtheta."""
+    import torch
+    from gpu_optical_photons_b200.adjoint import ResponseModel
+    from gpu_optical_photons_b200.params import TallyConfig, config2
+    from gpu_optical_photons_b200.wavefront import WaveConfig
+    base = config2()[0]
+    theta = (1000.0, 700.0, 0.95, 4.0)
+    tcal = TallyConfig(500, 50.0, 1)
+    m = ResponseModel(base, n, tcal, config=WaveConfig(math=math))
+    try:
+        w = torch.ones(tcal.time_bins + 1, dtype=torch.float64)
+        m.forward(theta)
+        m.replay(theta, w, 0.5)
+        fwd, adj = [], []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(); m.engine.run_tally(); b.record(); torch.cuda.synchronize()
+            fwd.append(a.elapsed_time(b))
+            a.record(); m.replay(theta, w, 0.5); b.record(); torch.cuda.synchronize()
+            adj.append(a.elapsed_time(b))
+    finally:
+        m.close()
+    f, r = float(np.median(fwd)), float(np.median(adj))
+    return {"forward_ms": f, "replay_ms": r, "replay_over_forward": r / f, "photons": n,
+            "setup": "Lambertian cube, Rayleigh, volume source, theta=(1000, 700, 0.95, 4), 500 time bins"}
 
 
 def run_reference(args):
@@ -415,6 +449,8 @@ def run_optx(args):
             other[m] = {"value": world * steps_of_tallies(t2) / (mm * 1e-3), "ms_per_step": mm,
                         "photon_steps_per_step": steps_of_tallies(t2)}
         line["other_math_modes"] = other
+    if not args.no_adjoint:
+        line["adjoint"] = adjoint_cost(args.math)
     if not args.no_history_baseline:
         hv, hms, ht = history_baseline(g, events, counts, tc, first_id, args.math, stream)
         # Same per-photon arithmetic, integer tallies: the two engines agree exactly.
