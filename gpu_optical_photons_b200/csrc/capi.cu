@@ -290,6 +290,7 @@ struct optx_engine {
   uint32_t n_tallies = 0;
   uint32_t ev_shift = kEvShift;
   bool gensteps = false;
+  bool uniform = false;  // every event has the same step physics (see same_step_physics)
   uint64_t total = 0;
   uint64_t first_id = 0;
   DevParams P0{};
@@ -299,7 +300,7 @@ struct optx_engine {
   bool timed = false;
   struct Graph {
     int mode;
-    bool batch;
+    int batch;  // WaveVariant
     int grid, block;
     size_t smem;
     DevParams P0;
@@ -312,7 +313,8 @@ struct optx_engine {
 
 namespace {
 
-size_t wave_smem(const optx_engine* e, int mode, bool batch) {
+size_t wave_smem(const optx_engine* e, int mode, int variant) {
+  const bool batch = variant != kSingle;
   const size_t pantry = static_cast<size_t>(e->cfg.block_size / 32) * kPantryBytesPerWarp;
   if (mode == kModeTally && !batch) return pantry + static_cast<size_t>(e->tdev.len - 7u) * 4u;
   if (mode == kModeAdjoint) return pantry + static_cast<size_t>(e->tdev.time_bins + 1u) * 8u;
@@ -330,7 +332,7 @@ int engine_minb(const optx_engine* e) {
   return std::max(2, std::min(4, b));
 }
 
-int engine_grid(optx_engine* e, int mode, bool batch, int& grid) {
+int engine_grid(optx_engine* e, int mode, int batch, int& grid) {
   const size_t smem = wave_smem(e, mode, batch);
   const int math = e->cfg.math;
   const int minb = engine_minb(e);
@@ -350,7 +352,7 @@ int engine_grid(optx_engine* e, int mode, bool batch, int& grid) {
 }
 
 // Writes the WaveArgs for a run (async on stream).
-int engine_upload_args(optx_engine* e, int mode, bool batch, int grid, cudaGraphConditionalHandle h,
+int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphConditionalHandle h,
                        const DevRecords* rec, const double* w_bin, double w_det,
                        const double* theta_inv, uint32_t score_mask, cudaStream_t st) {
   WaveArgs a;
@@ -410,9 +412,9 @@ int engine_upload_args(optx_engine* e, int mode, bool batch, int grid, cudaGraph
   return OPTX_OK;
 }
 
-int engine_graph(optx_engine* e, int mode, bool batch, int grid, optx_engine::Graph** out) {
+int engine_graph(optx_engine* e, int mode, int batch, int grid, optx_engine::Graph** out) {
   const size_t smem = wave_smem(e, mode, batch);
-  const DevParams P0 = batch ? DevParams{} : e->P0;
+  const DevParams P0 = batch == kBatch ? DevParams{} : e->P0;
   for (auto& g : e->graphs) {
     if (g.mode == mode && g.batch == batch && g.grid == grid && g.block == e->cfg.block_size &&
         g.smem == smem && std::memcmp(&g.P0, &P0, sizeof(P0)) == 0) {
@@ -481,8 +483,8 @@ int engine_graph(optx_engine* e, int mode, bool batch, int grid, optx_engine::Gr
 int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_bin, double w_det,
                const double* theta_inv, uint32_t score_mask, cudaStream_t st) {
   if (e->n_events == 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "no events uploaded");
-  // Gensteps always run batched: each lane reads its genstep's record.
-  const bool batch = e->n_events > 1 || e->gensteps;
+  // Gensteps always run batched: each lane reads its genstep's record at emission.
+  const int batch = (e->n_events > 1 || e->gensteps) ? (e->uniform ? kBatchUniform : kBatch) : kSingle;
   int grid = 0;
   OPTX_TRY(engine_grid(e, mode, batch, grid));
   const size_t smem = wave_smem(e, mode, batch);
@@ -501,7 +503,7 @@ int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_
     OPTX_CUDA(cudaEventRecord(e->ev0, st));
     OPTX_CUDA(DISPATCH(math, launch_wave_prep, e->d_args, e->d_ctrl,
                        std::max(1, std::min(grid, 4 * e->n_sm)), 256, st));
-    const DevParams P0 = batch ? DevParams{} : e->P0;
+    const DevParams P0 = batch == kBatch ? DevParams{} : e->P0;
     for (uint64_t w = 0;; ++w) {
       OPTX_CUDA(DISPATCH(math, launch_wave, mode, batch, engine_minb(e), P0, e->d_args, e->d_ctrl,
                          grid, e->cfg.block_size, smem, st));
@@ -1023,9 +1025,9 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
   };
   int grid_max = 0;
   for (int mode = 0; mode < 3; ++mode) {
-    for (int b = 0; b < 2; ++b) {
+    for (int b = kSingle; b <= kBatchUniform; ++b) {
       int g = 0;
-      const int rc = engine_grid(e, mode, b == 1, g);
+      const int rc = engine_grid(e, mode, b, g);
       if (rc != OPTX_OK && mode == kModeTally) return cleanup(rc);
       grid_max = std::max(grid_max, g);
     }
@@ -1094,6 +1096,18 @@ int optx_engine_destroy(optx_engine* e) {
 
 }  // extern "C"
 
+// True when two records have the same step physics (everything a step reads;
+// the source fields and tau act at emission only), bit for bit.
+static bool same_step_physics(DevParams a, DevParams b) {
+  for (DevParams* d : {&a, &b}) {
+    d->tau = 0.0f;
+    d->src_x = d->src_y = d->src_z = 0.0f;
+    d->source = 0u;
+    d->pad0 = d->pad1 = d->pad2 = 0u;
+  }
+  return std::memcmp(&a, &b, sizeof(DevParams)) == 0;
+}
+
 // Uploads the record table and offsets of the current batch and builds the
 // photon -> record table at the finest resolution the table holds.
 static int engine_upload_records(optx_engine* e, cudaStream_t st) {
@@ -1137,6 +1151,9 @@ int optx_engine_set_events(optx_engine* e, const optx_params* events, const optx
   e->n_events = n_events;
   e->n_tallies = n_events;
   e->gensteps = false;
+  e->uniform = true;
+  for (uint32_t i = 1; i < n_events && e->uniform; ++i)
+    e->uniform = same_step_physics(e->h_params[0], e->h_params[i]);
   e->total = total;
   e->first_id = first_id;
   e->P0 = e->h_params[0];
@@ -1190,6 +1207,8 @@ int optx_engine_set_gensteps(optx_engine* e, const optx_params* events, const op
   e->n_events = n_gensteps;
   e->n_tallies = n_events;
   e->gensteps = true;
+  e->uniform = true;
+  for (uint32_t i = 1; i < n_events && e->uniform; ++i) e->uniform = same_step_physics(ev[0], ev[i]);
   e->total = total;
   e->first_id = first_id;
   e->P0 = e->h_params[0];

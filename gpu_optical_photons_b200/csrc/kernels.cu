@@ -209,13 +209,14 @@ __global__ void wave_prep_kernel(const WaveArgs* __restrict__ A, WaveCtrl* __res
   }
 }
 
-// Physics of a lane's photon: the kernel argument (one configuration) or its
-// event's record in global memory, read field by field where the step uses it.
-// Lanes hold event indices; genstep records are read only at emission.
-template <bool BATCH>
+// Physics of a lane's photon: the kernel argument (one configuration, or a batch
+// whose events share their step physics: UNI) or its event's record in global
+// memory, read field by field where the step uses it. Lanes hold event indices;
+// records (events or gensteps) are read at emission only.
+template <bool BATCH, bool UNI>
 __device__ __forceinline__ const DevParams& params_of(const DevParams& P0,
                                                       const WaveArgs* __restrict__ A, uint32_t ev) {
-  if (BATCH) return A->phys[ev];
+  if (BATCH && !UNI) return A->phys[ev];
   return P0;
 }
 
@@ -225,7 +226,7 @@ __device__ __forceinline__ const DevParams& params_of(const DevParams& P0,
 template <int MINB>
 constexpr int wave_max_threads() { return MINB >= 5 ? 128 : 256; }
 
-template <int MODE, bool BATCH, int MINB>
+template <int MODE, bool BATCH, int MINB, bool UNI>
 __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(const DevParams P0,
                                                       const WaveArgs* __restrict__ A,
                                                       WaveCtrl* __restrict__ ctrl) {
@@ -499,7 +500,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
               na_aux.t_emit = d.y;
             }
             nev = __float_as_uint(d.z);
-            const DevParams& P = params_of<BATCH>(P0, A, nev);
+            const DevParams& P = params_of<BATCH, UNI>(P0, A, nev);
             nr.init(first_id + npidx, P.key_lo, P.key_hi, __float_as_uint(c.z));
           } else {
             const unsigned long long g = fresh_next + (item - n_in);
@@ -568,7 +569,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
             r.o = __float_as_uint(h.x);
             r.blk = __float_as_uint(h.y);
           }
-          const DevParams& P = params_of<BATCH>(P0, A, ev);
+          const DevParams& P = params_of<BATCH, UNI>(P0, A, ev);
           wsteps = 0u;
           alive = s.nb + s.ns < P.max_steps;
           if (!alive) finish(kMaxSteps, P);
@@ -592,7 +593,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
 
     // One step for every live lane.
     if (alive) {
-      const DevParams& P = params_of<BATCH>(P0, A, ev);
+      const DevParams& P = params_of<BATCH, UNI>(P0, A, ev);
       uint32_t fate = kMaxSteps;
       const bool still = step_photon<MODE == kModeAdjoint>(P, s, r, first_id + pidx, fate, aux);
       ++wsteps;
@@ -736,25 +737,34 @@ cudaError_t launch_wave_prep(const WaveArgs* A_dev, WaveCtrl* ctrl, int grid, in
   return cudaGetLastError();
 }
 
-template <int MODE, bool BATCH>
+template <int MODE, bool BATCH, bool UNI>
 static const void* kfn(int minb) {
   switch (minb) {
-    case 3: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 3>);
-    case 4: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 4>);
-    case 7: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 7>);
-    default: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 2>);
+    case 3: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 3, UNI>);
+    case 4: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 4, UNI>);
+    case 7: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 7, UNI>);
+    default: return reinterpret_cast<const void*>(&wave_kernel<MODE, BATCH, 2, UNI>);
   }
 }
 
-const void* wave_kernel_fn(int mode, bool batch, int minb) {
+template <int MODE>
+static const void* kfn_variant(int batch, int minb) {
+  switch (batch) {
+    case kBatchUniform: return kfn<MODE, true, true>(minb);
+    case kBatch: return kfn<MODE, true, false>(minb);
+    default: return kfn<MODE, false, false>(minb);
+  }
+}
+
+const void* wave_kernel_fn(int mode, int batch, int minb) {
   switch (mode) {
-    case kModeTally: return batch ? kfn<kModeTally, true>(minb) : kfn<kModeTally, false>(minb);
-    case kModeRecords: return batch ? kfn<kModeRecords, true>(minb) : kfn<kModeRecords, false>(minb);
-    default: return batch ? kfn<kModeAdjoint, true>(minb) : kfn<kModeAdjoint, false>(minb);
+    case kModeTally: return kfn_variant<kModeTally>(batch, minb);
+    case kModeRecords: return kfn_variant<kModeRecords>(batch, minb);
+    default: return kfn_variant<kModeAdjoint>(batch, minb);
   }
 }
 
-int wave_blocks_per_sm(int mode, bool batch, int minb, int block, size_t smem) {
+int wave_blocks_per_sm(int mode, int batch, int minb, int block, size_t smem) {
   int b = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, wave_kernel_fn(mode, batch, minb), block,
                                                     smem) != cudaSuccess)
@@ -762,12 +772,12 @@ int wave_blocks_per_sm(int mode, bool batch, int minb, int block, size_t smem) {
   return b;
 }
 
-cudaError_t wave_set_smem(int mode, bool batch, int minb, size_t smem) {
+cudaError_t wave_set_smem(int mode, int batch, int minb, size_t smem) {
   return cudaFuncSetAttribute(wave_kernel_fn(mode, batch, minb),
                               cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
 }
 
-cudaError_t launch_wave(int mode, bool batch, int minb, const DevParams& P, const WaveArgs* A_dev,
+cudaError_t launch_wave(int mode, int batch, int minb, const DevParams& P, const WaveArgs* A_dev,
                         WaveCtrl* ctrl, int grid, int block, size_t smem, cudaStream_t st) {
   void* args[] = {const_cast<DevParams*>(&P), &A_dev, &ctrl};
   return cudaLaunchKernel(wave_kernel_fn(mode, batch, minb), dim3(grid), dim3(block), args, smem, st);

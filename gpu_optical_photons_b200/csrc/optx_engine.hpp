@@ -74,6 +74,10 @@ struct WaveCtrl {
 };
 
 enum WaveMode : int { kModeTally = 0, kModeRecords = 1, kModeAdjoint = 2 };
+// Wave kernel variants: one configuration (physics in the kernel argument); a
+// batch of records with per-event physics; a batch whose events share their
+// step physics (kernel argument), with per-record emission and per-event tallies.
+enum WaveVariant : int { kSingle = 0, kBatch = 1, kBatchUniform = 2 };
 constexpr uint32_t kEvShift = 7;  // coarsest event-table resolution: one entry per 128 photons
 // Shared memory of one warp's pantry: 32 ready photons x 112 bytes (7 x 16 B;
 // the 112-byte stride makes 8 lanes' 128-bit accesses hit 8 distinct bank groups).
@@ -100,10 +104,11 @@ inline __host__ __device__ uint32_t slot_bin_bytes_per_warp(uint32_t n_bins) {
   cudaError_t launch_wave_prep(const WaveArgs* A_dev, WaveCtrl* ctrl, int grid, int block,       \
                                cudaStream_t st);                                                 \
   const void* wave_prep_fn();                                                                    \
-  const void* wave_kernel_fn(int mode, bool batch, int minb);                                    \
-  int wave_blocks_per_sm(int mode, bool batch, int minb, int block, size_t smem);                \
-  cudaError_t wave_set_smem(int mode, bool batch, int minb, size_t smem);                        \
-  cudaError_t launch_wave(int mode, bool batch, int minb, const DevParams& P,                    \
+  /* batch: kSingle, kBatch or kBatchUniform (see WaveVariant) */                               \
+  const void* wave_kernel_fn(int mode, int batch, int minb);                                     \
+  int wave_blocks_per_sm(int mode, int batch, int minb, int block, size_t smem);                 \
+  cudaError_t wave_set_smem(int mode, int batch, int minb, size_t smem);                         \
+  cudaError_t launch_wave(int mode, int batch, int minb, const DevParams& P,                     \
                           const WaveArgs* A_dev, WaveCtrl* ctrl, int grid, int block,            \
                           size_t smem, cudaStream_t st);                                         \
   cudaError_t launch_event_table(const unsigned long long* offsets, uint32_t n_events,           \

@@ -81,6 +81,34 @@ def test_batched_events_exact_equals_oracle(engine, oracle):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("math_mode", ["exact", "fast"])
+def test_batched_shared_physics_equals_oracle(engine, oracle, math_mode):
+    """Events with the same step physics but their own sources, decay times and
+    photon counts run the shared-physics batched variant; the per-event tallies
+    equal the oracle's (exact mode) or agree in detection (fast mode)."""
+    rng = np.random.default_rng(23)
+    base = P.SimParams(surface=P.LAMBERTIAN, reflectivity=0.93, n_det=1.5, scat_length=400.0,
+                       abs_length=1500.0)
+    events = [base.replace(src_x=float(rng.uniform(-20, 20)), src_y=float(rng.uniform(-20, 20)),
+                           src_z=float(rng.uniform(-20, 20)), tau=float(rng.uniform(1, 6)),
+                           source=P.VOLUME if i % 5 == 0 else P.POINT) for i in range(30)]
+    counts = rng.integers(0, 20_000, len(events))
+    c = P.TallyConfig(100, 50.0, 10)
+    eng = WavefrontEngine(c, len(events), int(counts.sum()), WaveConfig(math=math_mode))
+    eng.set_events(events, counts, first_id=321)
+    eng.run_tally()
+    got = eng.tallies()
+    eng.close()
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64) + np.uint64(321)
+    arr = (P.CSimParams * len(events))(*[e.to_c() for e in events])
+    ref = oracle.batch_tally(arr, offs, c, mode=oracle.PORTABLE if math_mode == "exact" else oracle.PLATFORM)
+    assert np.array_equal(got[:, :5].sum(1), counts)
+    if math_mode == "exact":
+        assert np.array_equal(got, ref)
+    else:
+        assert np.abs(got[:, 0].astype(np.int64) - ref[:, 0].astype(np.int64)).sum() <= 0.001 * counts.sum()
+
+
 @pytest.mark.parametrize("chunk", [32, 33, 1000, 65536])
 @pytest.mark.parametrize("bins", [(100, 10), (300, 12)])  # bins cached per warp / global bins
 def test_batched_tallies_independent_of_chunk(engine, oracle, chunk, bins):
