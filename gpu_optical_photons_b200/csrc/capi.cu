@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -62,6 +63,16 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 }
 
 constexpr float kSpeedOfLight = 299.792458f;  // mm/ns (hd.hpp:37 of the reference)
+
+// Host-side fault injection for tests (unset in normal use). OPTX_TEST_FAULT=alloc
+// makes the engine's device allocations fail as cudaMalloc does when the device
+// is out of memory; OPTX_TEST_FAULT=watchdog caps every wavefront run at one wave,
+// so a run that needs more waves ends through the device-side watchdog (the
+// error word of the control block) instead of finishing.
+bool test_fault(const char* what) {
+  const char* v = std::getenv("OPTX_TEST_FAULT");
+  return v != nullptr && std::strcmp(v, what) == 0;
+}
 
 int check_params(const optx_params* p, const optx_faces* f) {
   if (p == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "params must not be NULL");
@@ -404,6 +415,7 @@ int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphC
   const unsigned long long cap =
       4ull * (max_steps + 2ull) + 4ull * (e->total / per_wave) + 64ull;
   a.wave_cap = static_cast<uint32_t>(std::min<unsigned long long>(std::max(cap, 100000ull), 0xfffffff0ull));
+  if (test_fault("watchdog")) a.wave_cap = 1u;
   a.use_graph = (e->cfg.use_graph >= 0) ? 1u : 0u;
   a.chunk = e->cfg.chunk;
   (void)grid;
@@ -1038,6 +1050,8 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
   qcap = (qcap + 31) & ~uint64_t(31);
   e->qcap = static_cast<uint32_t>(qcap);
   auto alloc = [&](void** p, size_t bytes) -> int {
+    if (test_fault("alloc"))
+      return fail(OPTX_ERR_CUDA, "cudaMalloc: out of memory (injected by OPTX_TEST_FAULT=alloc)");
     const cudaError_t err = cudaMalloc(p, bytes);
     if (err != cudaSuccess) {
       cudaGetLastError();

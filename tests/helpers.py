@@ -111,3 +111,13 @@ def mirror_box_escape_fraction(n_scint, n_det):
         return 1.0
     s = n_det / n_scint
     return 1.0 - math.sqrt(1.0 - s * s)
+
+
+def check_tally_consistency(flat, c) -> None:
+    """Internal consistency of a flat tally: the arrival-time histogram (with its
+    overflow bin) and the hit map each count every detected photon once."""
+    flat = np.asarray(flat, dtype=np.uint64)
+    det = int(flat[0])
+    t0, x0 = 5, 5 + c.time_bins + 1
+    assert int(flat[t0:x0].sum()) == det, "time histogram != detected"
+    assert int(flat[x0:x0 + c.xy_bins * c.xy_bins].sum()) == det, "hit map != detected"

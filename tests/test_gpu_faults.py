@@ -1,0 +1,68 @@
+"""Failure detection without a GPU fault.
+
+Faults are injected on the host (OPTX_TEST_FAULT, read by liboptx at each
+call): an allocation that fails as cudaMalloc does when the device is out of
+memory, and a wavefront run capped at one wave so that it ends through the
+device-side watchdog (the control block's error word, read back by the host).
+Neither traps, faults nor hangs the GPU; after each, the same process runs the
+same work correctly. Invalid inputs are rejected on the host before any launch.
+"""
+import numpy as np
+import pytest
+
+from gpu_optical_photons_b200 import params as P
+from gpu_optical_photons_b200._lib import InvalidArgument, OptxError
+from gpu_optical_photons_b200.wavefront import WaveConfig, WavefrontEngine
+
+pytestmark = pytest.mark.gpu
+
+OPTX_ERR_CUDA, OPTX_ERR_WATCHDOG = 3, 6
+
+
+def test_injected_allocation_failure(engine, monkeypatch):
+    monkeypatch.setenv("OPTX_TEST_FAULT", "alloc")
+    with pytest.raises(OptxError) as e:
+        WavefrontEngine(P.TallyConfig(), 4, 100_000)
+    assert e.value.code == OPTX_ERR_CUDA and "out of memory" in str(e.value)
+    monkeypatch.delenv("OPTX_TEST_FAULT")
+    eng = WavefrontEngine(P.TallyConfig(), 4, 100_000)
+    eng.set_events([P.SimParams()], [1000])
+    eng.run_tally()
+    assert int(eng.tallies()[0, :5].sum()) == 1000
+    eng.close()
+
+
+def test_watchdog_ends_the_run_and_the_engine_recovers(engine, monkeypatch):
+    p, c = P.config2()
+    n = 200_000
+    eng = WavefrontEngine(c, 1, n, WaveConfig(cadence=2, math="exact"))  # needs many waves
+    eng.set_events([p], [n])
+    monkeypatch.setenv("OPTX_TEST_FAULT", "watchdog")
+    eng.run_tally()
+    with pytest.raises(OptxError) as e:
+        eng.tallies()
+    assert e.value.code == OPTX_ERR_WATCHDOG
+    monkeypatch.delenv("OPTX_TEST_FAULT")
+    eng.run_tally()  # the next run resets the control block
+    got = eng.tallies()[0]
+    eng.close()
+    _, ref, _ = engine.run_gpu_tally(p, c, n, math="exact")
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("bad", [
+    {"threshold": 33}, {"block_size": 96 + 1}, {"block_size": 512}, {"chunk": 8},
+    {"blocks_per_sm": 5}, {"blocks_per_sm": 7, "block_size": 64}])
+def test_invalid_engine_settings_rejected(engine, bad):
+    with pytest.raises(InvalidArgument):
+        WavefrontEngine(P.TallyConfig(), 1, 1000, WaveConfig(**bad))
+
+
+def test_invalid_parameters_rejected_before_launch(engine):
+    for p in (P.SimParams(hx=-1.0), P.SimParams(n_scint=0.0), P.SimParams(abs_length=0.0),
+              P.SimParams(tau=-1.0), P.SimParams(surface=7), P.SimParams(source=2)):
+        with pytest.raises(InvalidArgument):
+            engine.run_gpu_tally(p, P.TallyConfig(), 100)
+    # and the device keeps working
+    _, flat, _ = engine.run_gpu_tally(P.SimParams(), P.TallyConfig(), 1000)
+    assert flat[:5].sum() == 1000

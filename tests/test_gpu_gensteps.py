@@ -13,7 +13,7 @@ from gpu_optical_photons_b200 import gensteps as G
 from gpu_optical_photons_b200 import params as P
 from gpu_optical_photons_b200._lib import InvalidArgument
 from gpu_optical_photons_b200.wavefront import WaveConfig, WavefrontEngine
-from helpers import compare_histories
+from helpers import check_tally_consistency, compare_histories
 
 pytestmark = pytest.mark.gpu
 
@@ -44,6 +44,8 @@ def test_genstep_tallies_exact_equal_oracle(engine, oracle, cfg):
     ref, _ = oracle.genstep_run(events, g, TC, first_id=123, mode=oracle.PORTABLE)
     assert got.shape == (len(events), TC.length)
     assert np.array_equal(got, ref)
+    for row in got:
+        check_tally_consistency(row, TC)
 
 
 def test_genstep_records_exact_equal_oracle(engine, oracle):

@@ -6,7 +6,7 @@ import pytest
 
 from gpu_optical_photons_b200 import params as P
 from gpu_optical_photons_b200.wavefront import WaveConfig, WavefrontEngine, batched_events
-from helpers import compare_histories, chi2_two_sample, steps_of
+from helpers import check_tally_consistency, compare_histories, chi2_two_sample, steps_of
 
 pytestmark = pytest.mark.gpu
 
@@ -47,6 +47,7 @@ def test_wavefront_tally_equals_history_tally(engine, cfg, math_mode):
     st = eng.stats()
     eng.close()
     assert np.array_equal(fh, fw)
+    check_tally_consistency(fw, c)
     assert st["useful_lane_steps"] == int(fh[-2] + fh[-1] + fh[1])
 
 
@@ -79,6 +80,8 @@ def test_batched_events_exact_equals_oracle(engine, oracle):
     arr = (P.CSimParams * len(events))(*[e.to_c() for e in events])
     ref = oracle.batch_tally(arr, offs, c, mode=oracle.PORTABLE)
     assert np.array_equal(got, ref)
+    for row in got:
+        check_tally_consistency(row, c)
 
 
 @pytest.mark.parametrize("math_mode", ["exact", "fast"])
