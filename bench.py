@@ -460,7 +460,7 @@ def run_optx(args):
             "what": "one history-kernel launch (optx_tally_device) per event, back to back on one "
                     "stream; identical tallies checked",
             "speedup_of_value": value / (world * hv)}
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:  # the CPU baseline is an N=1 figure
         base, _ = cpu_reference_leg(events, counts, tc, max_events=min(1024, len(events)))
         line["cpu_baseline"] = base
     if rank == 0:
