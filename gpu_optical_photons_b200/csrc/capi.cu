@@ -280,7 +280,6 @@ struct optx_engine {
   uint64_t max_photons = 0;
   uint64_t ev_entries = 0;   // capacity of the photon -> record table
   int n_sm = 0;
-  size_t smem_tally = 0, smem_tally_batch = 0, smem_adj = 0;
   uint32_t qcap = 0;
   // device memory
   WaveArgs* d_args = nullptr;

@@ -1,7 +1,8 @@
 // kernels.cu - photon transport kernels for sm_100a.
 //
-// Compiled twice by the build: OPTX_NS=fast (CUDA libm, FMA contraction) and
-// OPTX_NS=exact (portable math, -fmad=false). Kernels:
+// Compiled three times by the build: OPTX_NS=fast (CUDA libm, FMA contraction),
+// OPTX_NS=exact (portable math, -fmad=false) and OPTX_NS=approx (the fast
+// source with --use_fast_math). Kernels:
 //
 //  * history_records_kernel / history_tally_kernel: one thread per photon for
 //    its whole history, the drop-in for the reference's transport_records_kernel
@@ -14,21 +15,23 @@
 //  * wave_kernel: the wavefront engine, the B200 form of the reference's
 //    event_step_kernel (src/gpu/gpu_event.cu:125-170). A persistent grid of warps
 //    keeps one photon per lane in registers. When fewer than `threshold` lanes of
-//    a warp are alive, the warp takes the next work items with one atomic
-//    (warp-aggregated) and the idle lanes load a survivor of the previous wave
-//    from the state queue or emit a fresh photon, so warps stay full instead of
-//    waiting for their longest history. When the wave's items are used up, or a
-//    photon has made `cadence` steps in this wave, the warp spills its live
-//    photons: ballot + popc give each one a slot after a single atomicAdd, and the
-//    state is written as 4 x 128-bit stores into an AoSoA queue tile (32 photons x
-//    64 B). The next wave (the next iteration of a CUDA-graph while loop, or the
-//    next host launch) reads them back with 4 x 128-bit coalesced loads. The
-//    last block to finish a wave sets up the next one (counters only; no block
-//    ever waits for another). Photons may belong to different events (batched
-//    mode): each lane then reads its event's 112-byte parameter record with
-//    7 x 128-bit loads per step, and tallies go to that event's slice.
+//    a warp are alive, the idle lanes take photons from the warp's shared-memory
+//    pantry, which all 32 lanes refill together (a fresh photon is emitted, or a
+//    survivor of the previous wave is loaded from the state queue) from a chunk
+//    of consecutive work items the warp claimed with one atomic. When the wave's
+//    items are used up, or a photon has made `cadence` steps in this wave, the
+//    warp spills its live photons: ballot + popc give each one a slot after a
+//    single atomicAdd, and the state is written as 4 x 128-bit stores into an
+//    AoSoA queue tile (32 photons x 64 B). The next wave (the next iteration of a
+//    CUDA-graph while loop, or the next host launch) reads them back with 4 x
+//    128-bit coalesced loads. The last block to finish a wave sets up the next one
+//    (counters only; no block ever waits for another).
+//    Variants: one configuration (physics in the kernel argument); a batch of
+//    records (events or gensteps) whose photons read their event's physics record
+//    per step; a batch whose events share their step physics (kernel argument).
+//    Batched tallies go through two per-warp shared-memory event slots.
 //    Records depend only on (seed, photon id), so they equal the history
-//    kernel's bit for bit for any block size, threshold, cadence or wave size.
+//    kernel's bit for bit for any block size, threshold, cadence, chunk or wave size.
 #include <cuda_runtime.h>
 
 #include "optx_device.cuh"

@@ -1,6 +1,6 @@
 // optx_engine.hpp - internal interface between the C ABI (capi.cu) and the
-// kernels (kernels.cu, compiled once per math mode into namespaces optx::fast
-// and optx::exact). Not part of the public ABI (include/optx.h is).
+// kernels (kernels.cu, compiled once per math mode into namespaces optx::fast,
+// optx::exact and optx::approx). Not part of the public ABI (include/optx.h is).
 #pragma once
 
 #include <cstdint>
