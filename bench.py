@@ -267,7 +267,43 @@ def run_reference(args):
             "cpu_baseline": {**base, "value": value,
                              "sample": f"{per_step} consecutive events per step; " + base["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    rg = reference_gpu_leg(events, counts, tc)
+    if rg is not None:
+        line["reference_gpu"] = rg
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_leg(events, counts, tc):
+    """The same batch through the reference's own GPU backend rebuilt for sm_100a
+    (oracle/_ref/libref_gpu.so: src/gpu/gpu_backend.cu compiled by nvcc from the
+    reference sources): one run_gpu_tally call per event, as the reference's API
+    processes events (each call allocates, launches, copies back and frees).
+    Informational, beside the CPU value; None without the library or a GPU."""
+    from oracle import oracle as O
+    try:
+        import torch
+        if not (O.refgpu_available() and torch.cuda.is_available()):
+            return None
+    except Exception:
+        return None
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+
+    def one_pass():
+        steps, kms = 0, 0.0
+        t0 = time.perf_counter()
+        for i, e in enumerate(events):
+            if counts[i]:
+                t, tm = O.refgpu_tally(e, tc, int(counts[i]), int(offs[i]))
+                steps += steps_of_tallies(t[None, :])
+                kms += tm["kernel_ms"]
+        return steps, (time.perf_counter() - t0) * 1e3, kms
+
+    one_pass()  # warm-up: context, module load, clocks
+    steps, wall_ms, kms = one_pass()
+    return {"value": steps / (wall_ms * 1e-3), "unit": UNIT, "ms_per_step": wall_ms,
+            "kernel_only_value": steps / (kms * 1e-3), "kernel_ms_per_step": kms, "calls": int((counts > 0).sum()),
+            "what": "reference src/gpu/gpu_backend.cu built for sm_100a from its sources; run_gpu_tally per event "
+                    "(host buffers, allocation per call), same 4096-event batch and tally binning"}
 
 
 def run_optx(args):

@@ -311,3 +311,70 @@ def compare_histories(a: Records, b: Records) -> dict:
     return {"n": n, "bitwise_identical": int(same_bits.sum()), "same_discrete": int(discrete.sum()),
             "fate_differs": int((a["fate"] != b["fate"]).sum()),
             "first_divergent": int(bad[0]) if len(bad) else -1}
+
+
+# ---- the reference's own GPU backend, rebuilt for sm_100a (oracle/_ref) --------
+
+REF_GPU_SO = {PLATFORM: os.path.join(HERE, "_ref", "libref_gpu.so"),
+              PORTABLE: os.path.join(HERE, "_ref", "libref_gpu_portable.so")}
+_refgpu = {}
+
+
+def refgpu_available(mode: int = PLATFORM) -> bool:
+    return os.path.exists(REF_GPU_SO[mode])
+
+
+def refgpu(mode: int = PLATFORM):
+    if mode not in _refgpu:
+        L = ctypes.CDLL(REF_GPU_SO[mode])
+        L.refgpu_available.restype = ctypes.c_int
+        L.refgpu_records.restype = ctypes.c_int
+        L.refgpu_records.argtypes = [_P, _u64, ctypes.c_int, _u64, _u64] + [_P] * 8 + [_P]
+        L.refgpu_tally.restype = ctypes.c_int
+        L.refgpu_tally.argtypes = [_P, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32, _u64, ctypes.c_int,
+                                   _u64, _P, _P]
+        L.refgpu_records_event.restype = ctypes.c_int
+        L.refgpu_records_event.argtypes = [_P, _u64, ctypes.c_uint32, ctypes.c_int, _u64, _u64] + [_P] * 8 + [_P, _P]
+        _refgpu[mode] = L
+    return _refgpu[mode]
+
+
+def _timing(t):
+    return dict(zip(("total_ms", "kernel_ms", "h2d_ms", "d2h_ms", "alloc_ms"), (float(v) for v in t)))
+
+
+def refgpu_records(p, n: int, first_id: int = 0, mode: int = PLATFORM, block_size: int = 256,
+                   chunk: int = 1 << 24):
+    """The reference's run_gpu_records (src/gpu/gpu_backend.cu) on this GPU."""
+    r = Records.empty(n)
+    cp = p.to_c()
+    t = np.zeros(5)
+    rc = refgpu(mode).refgpu_records(ctypes.byref(cp), n, block_size, first_id, chunk,
+                                     *[_ptr(r[k]) for k in Records.FIELDS], _ptr(t))
+    assert rc == 0, "reference run_gpu_records threw"
+    return r, _timing(t)
+
+
+def refgpu_tally(p, c, n: int, first_id: int = 0, mode: int = PLATFORM, block_size: int = 256):
+    """The reference's run_gpu_tally on this GPU: (flat tally, timing)."""
+    out = np.zeros(c.length, np.uint64)
+    cp = p.to_c()
+    t = np.zeros(5)
+    rc = refgpu(mode).refgpu_tally(ctypes.byref(cp), c.time_bins, c.time_max, c.xy_bins, n, block_size,
+                                   first_id, _ptr(out), _ptr(t))
+    assert rc == 0, "reference run_gpu_tally threw"
+    return out, _timing(t)
+
+
+def refgpu_records_event(p, n: int, k: int, first_id: int = 0, mode: int = PLATFORM, block_size: int = 256,
+                         chunk: int = 1 << 24):
+    """The reference's run_gpu_records_event (src/gpu/gpu_event.cu) on this GPU."""
+    r = Records.empty(n)
+    cp = p.to_c()
+    st = np.zeros(4)
+    t = np.zeros(5)
+    rc = refgpu(mode).refgpu_records_event(ctypes.byref(cp), n, k, block_size, first_id, chunk,
+                                           *[_ptr(r[k2]) for k2 in Records.FIELDS], _ptr(st), _ptr(t))
+    assert rc == 0, "reference run_gpu_records_event threw"
+    return r, {"launches": int(st[0]), "useful_lane_steps": int(st[1]), "issued_lane_steps": int(st[2]),
+               "kernels_ms": float(st[3])}, _timing(t)

@@ -18,6 +18,12 @@ Two flavours, as the reference's CMake options give them:
 
 each with gpu_tests, optphot, optphot_compare, optphot_event_bench, optphot_bench.
 
+It also builds the reference's own GPU backend (src/gpu/gpu_backend.cu,
+src/gpu/gpu_event.cu) for sm_100a with nvcc, in the same two flavours, behind a
+C wrapper (oracle/ref_gpu_capi.cpp): oracle/_ref/libref_gpu.so and
+libref_gpu_portable.so, to compare this repository's kernels with the
+reference kernels on the same B200.
+
     python oracle/relink.py [--ref DIR] [--force]
 """
 from __future__ import annotations
@@ -78,6 +84,37 @@ def _compile(args):
     subprocess.run(cmd, check=True)
 
 
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc")
+GPU_FLAVOURS = {
+    # the reference's CMake: -lineinfo, fmad on by default; OPTPHOT_CUDA_FMAD=OFF -> --fmad=false
+    "libref_gpu.so": [],
+    "libref_gpu_portable.so": ["-DOPTPHOT_PORTABLE_MATH", "-DOPTPHOT_NO_FMAD", "--fmad=false"],
+}
+
+
+def build_ref_gpu(ref: str = "/root/reference", force: bool = False) -> list[str]:
+    """The reference's GPU backend for sm_100a, one shared library per flavour."""
+    if not os.path.isdir(os.path.join(ref, "src", "gpu")):
+        return []
+    out_dir = os.path.join(HERE, "_ref")
+    os.makedirs(out_dir, exist_ok=True)
+    srcs = [os.path.join(ref, "src", "gpu", "gpu_backend.cu"), os.path.join(ref, "src", "gpu", "gpu_event.cu"),
+            os.path.join(HERE, "ref_gpu_capi.cpp"), os.path.join(ref, "src", "cpu", "cpu_backend.cpp")]
+    jobs = []
+    for name, flags in GPU_FLAVOURS.items():
+        lib = os.path.join(out_dir, name)
+        if force or _stale(lib, srcs + [os.path.join(HERE, "relink.py")]):
+            jobs.append([NVCC, "-shared", "-O3", "-std=c++17", "-lineinfo",
+                         "-gencode", "arch=compute_100a,code=sm_100a",
+                         "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", os.path.join(ref, "include")]
+                        + flags + srcs + ["-o", lib])
+    with ThreadPoolExecutor(max_workers=2) as pool:
+        for r in pool.map(lambda c: subprocess.run(c, check=False), jobs):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+    return [os.path.join(out_dir, n) for n in GPU_FLAVOURS]
+
+
 def build(ref: str = "/root/reference", force: bool = False) -> str | None:
     """Builds every program of both flavours; returns the output directory, or
     None when the reference checkout or liboptx.so is missing."""
@@ -117,6 +154,7 @@ def main(argv=None):
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args(argv)
+    build_ref_gpu(a.ref, a.force)
     out = build(a.ref, a.force)
     if out is None:
         print("reference checkout or liboptx.so missing: nothing built", file=sys.stderr)
