@@ -434,6 +434,7 @@ def run_optx(args):
                               "wave_quota": cfg.wave_quota,
                               "blocks_per_sm": cfg.blocks_per_sm,
                               "cadence": cfg.cadence, "chunk": cfg.chunk or 256,
+                              "tail_steps": cfg.tail_steps or 4096,
                               "graph": cfg.use_graph, "math": cfg.math},
                    "parallelism": f"dp{world} (independent event batches per GPU)"},
         "e2e": {"value": world * steps_per_run / (e2e_step * 1e-3), "unit": UNIT,

@@ -64,7 +64,8 @@ class CWaveConfig(ctypes.Structure):
                 ("threshold", ctypes.c_uint32), ("cadence", ctypes.c_uint32),
                 ("wave_quota", ctypes.c_uint64), ("use_graph", ctypes.c_int32),
                 ("math", ctypes.c_int32), ("chunk", ctypes.c_uint32),
-                ("max_gensteps", ctypes.c_uint32)]
+                ("max_gensteps", ctypes.c_uint32), ("tail_steps", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class CGenstep(ctypes.Structure):

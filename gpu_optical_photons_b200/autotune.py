@@ -14,11 +14,14 @@ a tally configuration), the engine settings by measurement on the device:
 * ``chunk`` — consecutive photons a warp claims with one atomic (larger keeps a
   warp on one event longer, so its shared-memory tally slots hit more often;
   smaller balances the end of a wave better);
+* ``tail_steps`` — steps a photon makes in a wave before the end-of-wave
+  compaction may move it to the next wave (large: warps keep their photons
+  until they finish, one wave per run);
 * ``wave_quota`` — fresh photons admitted per wave, i.e. the depth of the work
   queue between two compactions (0 = all photons in the first wave).
 
 Staged coordinate search: (blocks_per_sm x threshold) first, then block size,
-cadence, chunk and queue depth around the best point. Each candidate is timed with
+cadence, chunk, tail steps and queue depth around the best point. Each candidate is timed with
 CUDA events on the launching stream (median of `repeats` runs after one warm-up
 run), on the real workload. Every candidate computes the same tallies (the
 engine's results do not depend on these settings), which `tune` checks.
@@ -60,7 +63,7 @@ def time_config(cfg: WaveConfig, events, counts, tally: TallyConfig, repeats: in
 
 def tune(events, counts, tally: TallyConfig, base: WaveConfig | None = None, repeats: int = 3,
          bps=(2, 3, 4, 7), thresholds=(16, 20, 24, 28, 32), blocks=(128, 256), cadences=(0, 32),
-         quota_fracs=(0.0, 0.25), chunks=(64, 256, 1024), verbose: bool = False):
+         quota_fracs=(0.0, 0.25), chunks=(64, 256, 1024), tails=(64, 4096), verbose: bool = False):
     """Returns (best WaveConfig, list of measurement dicts)."""
     base = base or WaveConfig()
     total = int(np.sum(counts))
@@ -106,6 +109,13 @@ def tune(events, counts, tally: TallyConfig, base: WaveConfig | None = None, rep
         if ch == (best_cfg.chunk or 256):
             continue
         cfg = replace(best_cfg, chunk=ch)
+        ms = measure(cfg)
+        if ms < best_ms:
+            best_cfg, best_ms = cfg, ms
+    for tl in tails:
+        if tl == (best_cfg.tail_steps or 4096):
+            continue
+        cfg = replace(best_cfg, tail_steps=tl)
         ms = measure(cfg)
         if ms < best_ms:
             best_cfg, best_ms = cfg, ms

@@ -417,6 +417,7 @@ int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphC
   if (test_fault("watchdog")) a.wave_cap = 1u;
   a.use_graph = (e->cfg.use_graph >= 0) ? 1u : 0u;
   a.chunk = e->cfg.chunk;
+  a.tail_steps = e->cfg.tail_steps;
   (void)grid;
   (void)batch;
   OPTX_CUDA(cudaMemcpyAsync(e->d_args, &a, sizeof(a), cudaMemcpyHostToDevice, st));
@@ -1014,6 +1015,8 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
   if (k.threshold > 32) return fail(OPTX_ERR_INVALID_ARGUMENT, "threshold must be 1..32");
   if (k.use_graph == 0) k.use_graph = 1;
   if (k.chunk == 0) k.chunk = 256;
+  if (k.tail_steps == 0) k.tail_steps = 4096;
+  if (k.reserved != 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "reserved must be 0");
   if (k.chunk < 32 || k.chunk > (1u << 20))
     return fail(OPTX_ERR_INVALID_ARGUMENT, "chunk must be in [32, 2^20]");
   if (k.max_gensteps > (1u << 30)) return fail(OPTX_ERR_INVALID_ARGUMENT, "max_gensteps must be <= 2^30");
@@ -1520,6 +1523,7 @@ extern "C" int optx_wavefront_tally_noalloc(const optx_params* p, const optx_fac
   a.tc = td;
   a.use_graph = 0u;
   a.chunk = 256u;
+  a.tail_steps = 4096u;
   a.iter_cap = (static_cast<unsigned long long>(n) + a.qcap + 64ull) * (P.max_steps + 2ull) + 4096ull;
   a.wave_cap = static_cast<uint32_t>(std::min<unsigned long long>(
       std::max<unsigned long long>(4ull * (P.max_steps + 2ull) + 64ull, 100000ull), 0xfffffff0ull));

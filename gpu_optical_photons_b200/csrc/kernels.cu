@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     const float4* qin;
     float4* qout;
     unsigned long long fresh_next, first_id, iter_cap;
-    uint32_t n_in, items, T, cadence, qcap, chunk, ev_shift;
+    uint32_t n_in, items, T, cadence, qcap, chunk, ev_shift, tail_steps;
     const uint32_t* tally_of;
     TallyDev tc;
   };
@@ -274,6 +274,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     ws.chunk = A->chunk < 32u ? 32u : A->chunk;
     ws.tally_of = A->tally_of;
     ws.ev_shift = A->ev_shift;
+    ws.tail_steps = A->tail_steps < 1u ? 1u : A->tail_steps;
     ws.tc = A->tc;
   }
   __syncthreads();
@@ -286,6 +287,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
   const unsigned long long& first_id = ws.first_id;
   const unsigned long long& iter_cap = ws.iter_cap;
   const uint32_t& wchunk = ws.chunk;
+  const uint32_t& tail_steps = ws.tail_steps;
   // Event of a record (a genstep's event; a plain batch's records are its events).
   auto event_of = [&](uint32_t rec) -> uint32_t {
     const uint32_t* m = ws.tally_of;
@@ -317,7 +319,6 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
   uint32_t pidx = 0u, ev = 0u;
   bool alive = false;
   bool exhausted = false;  // warp-uniform: the wave's work items are all handed out
-  bool refilled = false;   // warp-uniform: lanes were loaded and have not stepped yet
   uint32_t pc = 0u;        // warp-uniform: photons waiting in this warp's pantry
   uint32_t wsteps = 0u;
   // Work items [chunk_lo, chunk_hi) claimed by this warp and not yet emitted (warp-uniform).
@@ -578,17 +579,18 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
           if (!alive) finish(kMaxSteps, P);
         }
         pc -= take;
-        refilled = true;
         __syncwarp();
         amask = __ballot_sync(kFull, alive);
         na = static_cast<uint32_t>(__popc(amask));
       }
       if (exhausted && pc == 0u) {
         if (na == 0u) break;
-        // Spill only photons that have stepped in this wave, so that every item
-        // of a wave makes progress and the run always ends.
-        if (na < T && !refilled && !queue_full) {
-          if (spill_lanes(alive)) alive = false;
+        // A photon moves on to the next wave (compaction into fuller warps) only
+        // after `tail_steps` (>= 1) steps in this one: every item of a wave makes
+        // progress, so the run ends, and long histories advance many steps per
+        // wave instead of one step per wave once the waves are small.
+        if (na < T && !queue_full) {
+          if (spill_lanes(alive && wsteps >= tail_steps)) alive = false;
           if (__ballot_sync(kFull, alive) == 0u) break;
         }
       }
@@ -608,7 +610,6 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
         finish(kMaxSteps, P);
       }
     }
-    refilled = false;
     ++iters;
     useful += na;
     if (cadence != 0u && !queue_full) {  // forced compaction after `cadence` steps in this wave

@@ -52,7 +52,7 @@ struct WaveArgs {
   uint32_t chunk;                       // consecutive work items a warp claims per grab (>= 32)
   uint32_t n_tallies;                   // events = tally slices (= n_events unless gensteps)
   uint32_t ev_shift;                    // ev_table resolution: one entry per 2^ev_shift photons
-  uint32_t pad3;
+  uint32_t tail_steps;                  // steps a photon makes in a wave before it may be spilled at its end
   const uint32_t* tally_of;             // record -> event (null: the record's own index)
   const float4* seg;                    // genstep records: 2 float4 each (end x,y,z,t0), (dt,-,-,-)
 };

@@ -108,6 +108,10 @@ typedef struct optx_wave_config {
   uint32_t chunk;        /* consecutive photons a warp claims per grab, 32..2^20 (default 256);
                             results do not depend on it */
   uint32_t max_gensteps; /* capacity for optx_engine_set_gensteps, 0 = none (default) */
+  uint32_t tail_steps;   /* at the end of a wave a photon moves on to the next wave only after
+                            this many steps in the wave (default 4096: in practice a warp keeps its
+                            photons until they finish); results do not depend on it */
+  uint32_t reserved;     /* must be 0 */
 } optx_wave_config;
 
 /* Extension (no reference counterpart; the reference lists generation on the GPU

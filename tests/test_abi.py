@@ -57,7 +57,7 @@ def test_struct_layouts():
     assert ctypes.sizeof(_lib.CRecords) == 64
     assert ctypes.sizeof(_lib.CTiming) == 40
     assert ctypes.sizeof(_lib.CEventStats) == 40
-    assert ctypes.sizeof(_lib.CWaveConfig) == 40
+    assert ctypes.sizeof(_lib.CWaveConfig) == 48
     assert ctypes.sizeof(_lib.CGenstep) == 40
 
 
