@@ -637,9 +637,11 @@ void parallel_copy(const std::vector<std::tuple<void*, const void*, size_t>>& jo
 // per-photon arithmetic as the history kernels (bit-identical records, equal
 // integer tallies) at 1.4-2x their speed on one configuration. One engine per
 // (device, math mode, tally configuration, photon capacity) is created on first
-// use and kept until optx_release_cache; its mutex serialises a call's upload /
-// run / read-back sequence. Lock order: g_pipe_mu, then an engine's mu, then g_mu
-// (taken inside the optx_engine_* calls).
+// use; the most recent kApiMaxEngines are kept (until optx_release_cache). A call
+// holds a reference to its engine, so an engine dropped from the cache lives until
+// its last call ends; its mutex serialises a call's upload / run / read-back
+// sequence. Lock order: g_pipe_mu, then an engine's mu, then g_mu (taken inside
+// the optx_engine_* calls).
 struct ApiEngine {
   int device = -1;
   int math = 0;
@@ -647,8 +649,12 @@ struct ApiEngine {
   uint64_t cap = 0;
   optx_engine* e = nullptr;
   std::mutex mu;
+  ~ApiEngine() { optx_engine_destroy(e); }
 };
-std::vector<std::unique_ptr<ApiEngine>> g_api;  // guarded by g_mu
+// Guarded by g_mu, oldest first. Never destroyed: at process exit the CUDA
+// runtime may already be gone, so cached engines are not freed then.
+std::vector<std::shared_ptr<ApiEngine>>& g_api = *new std::vector<std::shared_ptr<ApiEngine>>();
+constexpr size_t kApiMaxEngines = 8;
 std::mutex g_pipe_mu;                           // the records pipeline (g_pipe)
 constexpr uint64_t kApiMaxCap = 1ull << 27;     // photons per engine run
 
@@ -662,7 +668,7 @@ uint64_t api_capacity(uint64_t n) {
 
 // Finds or creates the engine. OPTX_ERR_RUNTIME means the wave kernel cannot be
 // resident beside these histograms (the caller then runs the history kernel).
-int api_engine(int math, const optx_tally_config& tc, uint64_t cap, ApiEngine** out) {
+int api_engine(int math, const optx_tally_config& tc, uint64_t cap, std::shared_ptr<ApiEngine>& out) {
   int dev = 0;
   OPTX_CUDA(cudaGetDevice(&dev));
   auto match = [&](const ApiEngine& a) {
@@ -673,7 +679,7 @@ int api_engine(int math, const optx_tally_config& tc, uint64_t cap, ApiEngine** 
     std::lock_guard<std::mutex> lk(g_mu);
     for (auto& a : g_api)
       if (match(*a)) {
-        *out = a.get();
+        out = a;
         return OPTX_OK;
       }
   }
@@ -685,14 +691,19 @@ int api_engine(int math, const optx_tally_config& tc, uint64_t cap, ApiEngine** 
   cfg.math = math;
   optx_engine* e = nullptr;
   OPTX_TRY(optx_engine_create(&tc, 1, cap, &cfg, &e));
-  auto a = std::make_unique<ApiEngine>();
+  auto a = std::make_shared<ApiEngine>();
   a->device = dev;
   a->math = math;
   a->tc = tc;
   a->cap = cap;
   a->e = e;
+  out = a;
+  std::shared_ptr<ApiEngine> dropped;  // released after g_mu
   std::lock_guard<std::mutex> lk(g_mu);
-  *out = a.get();
+  if (g_api.size() >= kApiMaxEngines) {
+    dropped = g_api.front();
+    g_api.erase(g_api.begin());
+  }
   g_api.push_back(std::move(a));
   return OPTX_OK;
 }
@@ -729,7 +740,7 @@ int optx_gpu_device_name(char* buf, size_t len) {
 const char* optx_last_error(void) { return g_err.c_str(); }
 
 int optx_release_cache(void) {
-  std::vector<std::unique_ptr<ApiEngine>> engines;
+  std::vector<std::shared_ptr<ApiEngine>> engines;  // destroyed after g_mu, once unused
   {
     std::lock_guard<std::mutex> lk(g_mu);
     if (g_cache.rec) cudaFree(g_cache.rec);
@@ -739,10 +750,7 @@ int optx_release_cache(void) {
     g_cache = Cache{};
     engines.swap(g_api);
   }
-  for (auto& a : engines) {  // wait for calls still using an engine
-    std::lock_guard<std::mutex> lk(a->mu);
-    optx_engine_destroy(a->e);
-  }
+  engines.clear();  // an engine still used by a call is destroyed when that call ends
   return OPTX_OK;
 }
 
@@ -770,9 +778,9 @@ int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
   OPTX_TRY(pipe_ensure(cap));
   // The wavefront engine writes each chunk's records (the history kernel when the
   // engine cannot be created, which a records run never needs in practice).
-  ApiEngine* ae = nullptr;
+  std::shared_ptr<ApiEngine> ae;
   const optx_tally_config no_tally{1u, 1.0f, 1u};
-  const int erc = api_engine(math, no_tally, api_capacity(cap), &ae);
+  const int erc = api_engine(math, no_tally, api_capacity(cap), ae);
   if (erc != OPTX_OK && erc != OPTX_ERR_RUNTIME) return erc;
   std::unique_lock<std::mutex> elk;
   if (erc == OPTX_OK) elk = std::unique_lock<std::mutex>(ae->mu);
@@ -867,8 +875,8 @@ int optx_run_tally(const optx_params* p, const optx_faces* faces, const optx_tal
   const auto t0 = std::chrono::steady_clock::now();
   if (n > 0) {
     // The wavefront engine, in runs of at most its capacity, tallies summed on the host.
-    ApiEngine* ae = nullptr;
-    const int erc = api_engine(math, *c, api_capacity(n), &ae);
+    std::shared_ptr<ApiEngine> ae;
+    const int erc = api_engine(math, *c, api_capacity(n), ae);
     if (erc != OPTX_OK && erc != OPTX_ERR_RUNTIME) return erc;
     if (erc == OPTX_OK) {
       tm.alloc_ms = ms_since(t0);

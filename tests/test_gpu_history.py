@@ -206,3 +206,38 @@ def test_records_pipeline_pinned_and_pageable(engine):
     assert compare_histories(rec2, want)["bitwise_identical"] == n
     small, _ = engine.run_gpu_records(p, 1000, first_id=3, chunk=77)  # many tiny chunks
     assert compare_histories(small, {k: v[:1000] for k, v in want.items()})["bitwise_identical"] == 1000
+
+
+def test_host_call_engine_cache_eviction(engine):
+    """Host tally calls with more tally configurations than the engine cache holds
+    (8), interleaved: every result equals the device history kernel's."""
+    p = P.config2()[0]
+    for i in range(12):
+        c = P.TallyConfig(50 + 7 * i, 50.0, 3 + i % 4)
+        _, flat, _ = engine.run_gpu_tally(p, c, 50_000, first_id=i)
+        dev = engine.tally_device(p, c, 50_000, first_id=i)
+        assert np.array_equal(flat, dev.cpu().numpy().astype(np.uint64)), i
+    from gpu_optical_photons_b200 import _lib
+    assert _lib.lib().optx_release_cache() == 0
+    _, flat, _ = engine.run_gpu_tally(p, P.TallyConfig(), 10_000)  # a fresh engine after release
+    assert flat[:5].sum() == 10_000
+
+
+def test_host_calls_from_several_threads(engine):
+    """Concurrent host calls (tally and records, two tally configurations) from
+    four threads give the results of the same calls made one at a time."""
+    from concurrent.futures import ThreadPoolExecutor
+    p = P.config2()[0]
+    cs = [P.TallyConfig(100, 50.0, 10), P.TallyConfig(200, 40.0, 5)]
+
+    def job(i):
+        if i % 3 == 2:
+            rec, _ = engine.run_gpu_records(p, 40_000, first_id=i)
+            return ("rec", i, int(rec["n_boundary"].sum()), int(rec["fate"].astype(np.int64).sum()))
+        _, flat, _ = engine.run_gpu_tally(p, cs[i % 2], 60_000, first_id=i)
+        return ("tally", i, flat.tobytes())
+
+    serial = [job(i) for i in range(12)]
+    with ThreadPoolExecutor(4) as pool:
+        parallel = list(pool.map(job, range(12)))
+    assert serial == parallel
