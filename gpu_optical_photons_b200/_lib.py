@@ -98,6 +98,7 @@ _SIGS = {
     "optx_engine_run_tally": [_P, _P],
     "optx_engine_run_records": [_P, _P, _P],
     "optx_engine_run_adjoint": [_P, _P, ctypes.c_double, _P, _P],
+    "optx_engine_run_score_moments": [_P, _P, _P],
     "optx_wavefront_tally_noalloc": [_P, _P, _P, _u64, _u64, _P, _int, _P],
     "optx_engine_tally_ptr": [_P, _P, _P],
     "optx_engine_get_tallies": [_P, _P, _P],

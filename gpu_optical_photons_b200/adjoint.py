@@ -79,6 +79,20 @@ class ResponseModel:
                   float(w_det), ctypes.c_void_p(grad.data_ptr()), ctypes.c_void_p(stream))
         return grad.cpu().numpy()
 
+    def score_moments(self, theta) -> tuple[np.ndarray, np.ndarray]:
+        """(histogram h incl. overflow, Jacobian J) at theta from one replay.
+
+        J[b, j] = sum over photons detected in bin b of S_j, an unbiased estimate
+        of dE[h_b]/dtheta_j; h comes from the same photons (exact integer counts)."""
+        self._upload(theta)
+        tb = self.tally.time_bins
+        m = torch.empty((tb + 1) * 5, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        _lib.call("optx_engine_run_score_moments", self.engine._h, ctypes.c_void_p(m.data_ptr()),
+                  ctypes.c_void_p(stream))
+        M = m.view(tb + 1, 5).cpu().numpy()
+        return M[:, 0].copy(), M[:, 1:].copy()
+
     def close(self):
         self.engine.close()
 
@@ -161,6 +175,47 @@ def nll_loss(theta: torch.Tensor, model: ResponseModel, target: torch.Tensor) ->
     return poisson_nll(h, target, model.n, model.tally.time_bins)
 
 
+def _phi_of(theta) -> np.ndarray:
+    t = np.asarray(theta, np.float64)
+    return np.array([math.log(t[0]), math.log(t[1]), math.log(1.0 - t[2]), math.log(t[3])])
+
+
+def _theta_of(phi) -> np.ndarray:
+    e = np.exp(np.asarray(phi, np.float64))
+    return np.array([e[0], e[1], 1.0 - e[2], e[3]])
+
+
+def _dtheta_dphi(theta) -> np.ndarray:
+    t = np.asarray(theta, np.float64)
+    return np.array([t[0], t[1], -(1.0 - t[2]), t[3]])
+
+
+def fisher_information(hist: np.ndarray, jac: np.ndarray, theta, bins: int) -> np.ndarray:
+    """Poisson Fisher information of the first `bins` histogram bins with respect
+    to phi = (log La, log Ls, log(1-R), log tau):
+        F = sum_b (d lambda_b/d phi)(d lambda_b/d phi)^T / lambda_b,
+    lambda_b = h_b + 1, d lambda/d phi from the score Jacobian."""
+    Jp = jac[:bins] * _dtheta_dphi(theta)
+    lam = hist[:bins] + 1.0
+    return (Jp.T / lam) @ Jp
+
+
+def parameter_errors(model: "ResponseModel", theta, n_target: int | None = None) -> np.ndarray:
+    """One-sigma statistical errors of theta fitted to a target histogram of
+    n_target photons with a model of model.n photons: the inverse Fisher
+    information of the target's Poisson counts, inflated by (1 + n_target/n)
+    for the model's own sampling noise, mapped from phi to theta."""
+    hist, jac = model.score_moments(theta)
+    bins = model.tally.time_bins
+    F = fisher_information(hist, jac, theta, bins)
+    on = np.diag(F) > 0
+    cov = np.zeros((4, 4))
+    cov[np.ix_(on, on)] = np.linalg.inv(F[np.ix_(on, on)])
+    nt = model.n if n_target is None else n_target
+    cov *= 1.0 + nt / model.n
+    return np.sqrt(np.diag(cov)) * np.abs(_dtheta_dphi(theta))
+
+
 def _to_theta(phi: torch.Tensor) -> torch.Tensor:
     # phi = (log La, log Ls, log(1 - R), log tau): unconstrained and well scaled
     e = torch.exp(phi)
@@ -168,12 +223,32 @@ def _to_theta(phi: torch.Tensor) -> torch.Tensor:
 
 
 def calibrate(base: SimParams, theta0, target: np.ndarray, n: int, steps: int = 20,
-              lr: float = 0.04, model: ResponseModel | None = None):
-    """Adam on phi = (log La, log Ls, log(1-R), log tau) minimising the Poisson NLL
-    of the arrival-time histogram; gradients from the adjoint replay. Returns the
-    trajectory [(theta, loss)] including the final point."""
+              lr: float | None = None, model: ResponseModel | None = None, method: str = "fisher"):
+    """Fits theta to a target arrival-time histogram by minimising its Poisson NLL.
+
+    method "fisher": Fisher scoring (natural-gradient descent) on
+    phi = (log La, log Ls, log(1-R), log tau): each step runs one score-moment
+    replay, which gives the histogram, the gradient g = sum_b (1 - k_b/lambda_b)
+    d lambda_b/d phi and the Fisher information F, and moves phi by
+    -lr (F + 1e-6 diag F)^-1 g (lr 1; each component limited to 0.25 per step).
+    The Monte Carlo noise of the model makes the iterates wander inside the
+    target's error ellipse once they reach it, so the estimate is the average of
+    phi over the second half of the steps (Polyak-Ruppert averaging).
+    Trajectory: [(theta_i, loss_i)] for i = 0..steps, then (estimate, its loss).
+    method "adam": Adam (lr 0.04) on phi with gradients from the adjoint replay
+    through the autograd Function; trajectory [(theta_i, loss_i)] for
+    i = 0..steps, the last being the estimate. loss = the NLL per photon."""
     own = model is None
     model = model or ResponseModel(base, n)
+    if method == "fisher":
+        try:
+            return _calibrate_fisher(model, theta0, target, steps, 1.0 if lr is None else lr)
+        finally:
+            if own:
+                model.close()
+    if method != "adam":
+        raise ValueError(f"unknown method {method!r}")
+    lr = 0.04 if lr is None else lr
     tgt = torch.as_tensor(target, dtype=torch.float64)
     t0 = np.asarray(theta0, np.float64)
     phi = torch.tensor([math.log(t0[0]), math.log(t0[1]), math.log(1.0 - t0[2]), math.log(t0[3])],
@@ -194,4 +269,31 @@ def calibrate(base: SimParams, theta0, target: np.ndarray, n: int, steps: int = 
     finally:
         if own:
             model.close()
+    return traj
+
+
+def _calibrate_fisher(model: ResponseModel, theta0, target: np.ndarray, steps: int, lr: float,
+                      max_step: float = 0.25):
+    bins = model.tally.time_bins
+    k = np.asarray(target, np.float64)[:bins]
+    phi = _phi_of(theta0)
+    traj, phis = [], []
+    for it in range(steps + 2):
+        if it == steps + 1:  # the estimate: iterates steps/2 .. steps averaged
+            phi = np.mean(phis[steps // 2:], axis=0)
+        theta = _theta_of(phi)
+        hist, jac = model.score_moments(theta)
+        lam = hist[:bins] + 1.0
+        traj.append((theta.copy(), float((lam - k * np.log(lam)).sum() / model.n)))
+        phis.append(phi.copy())
+        if it >= steps:
+            continue
+        Jp = jac[:bins] * _dtheta_dphi(theta)
+        g = ((1.0 - k / lam)[:, None] * Jp).sum(0)
+        F = (Jp.T / lam) @ Jp
+        on = np.diag(F) > 0
+        d = np.zeros(4)
+        Fa = F[np.ix_(on, on)]
+        d[on] = np.linalg.solve(Fa + 1e-6 * np.diag(np.diag(Fa)), g[on])
+        phi = phi - np.clip(lr * d, -max_step, max_step)
     return traj

@@ -323,11 +323,13 @@ struct optx_engine {
 
 namespace {
 
-size_t wave_smem(const optx_engine* e, int mode, int variant) {
+size_t wave_smem(const optx_engine* e, int mode, int variant, bool moments = false) {
   const bool batch = variant != kSingle;
   const size_t pantry = static_cast<size_t>(e->cfg.block_size / 32) * kPantryBytesPerWarp;
   if (mode == kModeTally && !batch) return pantry + static_cast<size_t>(e->tdev.len - 7u) * 4u;
-  if (mode == kModeAdjoint) return pantry + static_cast<size_t>(e->tdev.time_bins + 1u) * 8u;
+  if (mode == kModeAdjoint)  // bin weights, then (score-moment runs) the block's moment table
+    return pantry + static_cast<size_t>(e->tdev.time_bins + 1u) * 8u +
+           (moments ? moment_smem_bytes(e->tdev.time_bins) : 0u);
   if (mode == kModeTally && batch)  // per-warp event slots
     return pantry + static_cast<size_t>(e->cfg.block_size / 32) *
                         (kSlotCounterBytesPerWarp + slot_bin_bytes_per_warp(e->tdev.len - 7u));
@@ -342,8 +344,8 @@ int engine_minb(const optx_engine* e) {
   return std::max(2, std::min(4, b));
 }
 
-int engine_grid(optx_engine* e, int mode, int batch, int& grid) {
-  const size_t smem = wave_smem(e, mode, batch);
+int engine_grid(optx_engine* e, int mode, int batch, int& grid, bool moments = false) {
+  const size_t smem = wave_smem(e, mode, batch, moments);
   const int math = e->cfg.math;
   const int minb = engine_minb(e);
   int dev = 0, max_smem = 0;
@@ -364,7 +366,8 @@ int engine_grid(optx_engine* e, int mode, int batch, int& grid) {
 // Writes the WaveArgs for a run (async on stream).
 int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphConditionalHandle h,
                        const DevRecords* rec, const double* w_bin, double w_det,
-                       const double* theta_inv, uint32_t score_mask, cudaStream_t st) {
+                       const double* theta_inv, uint32_t score_mask, cudaStream_t st,
+                       double* moments = nullptr) {
   WaveArgs a;
   std::memset(&a, 0, sizeof(a));
   a.params = e->d_params;
@@ -401,6 +404,8 @@ int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphC
   }
   a.score_mask = score_mask;
   a.grad = (mode == kModeAdjoint) ? e->d_grad : nullptr;
+  a.moments = (mode == kModeAdjoint) ? moments : nullptr;
+  a.moments_smem = (a.moments != nullptr && moment_smem_bytes(e->tdev.time_bins) != 0u) ? 1u : 0u;
   a.graph_handle = h;
   // Watchdog: no warp can iterate more than (photons + queue) x (max_steps + 2) times.
   uint32_t max_steps = 0;
@@ -424,8 +429,9 @@ int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphC
   return OPTX_OK;
 }
 
-int engine_graph(optx_engine* e, int mode, int batch, int grid, optx_engine::Graph** out) {
-  const size_t smem = wave_smem(e, mode, batch);
+int engine_graph(optx_engine* e, int mode, int batch, int grid, optx_engine::Graph** out,
+                 bool moments = false) {
+  const size_t smem = wave_smem(e, mode, batch, moments);
   const DevParams P0 = batch == kBatch ? DevParams{} : e->P0;
   for (auto& g : e->graphs) {
     if (g.mode == mode && g.batch == batch && g.grid == grid && g.block == e->cfg.block_size &&
@@ -493,25 +499,26 @@ int engine_graph(optx_engine* e, int mode, int batch, int grid, optx_engine::Gra
 
 // One complete run of the uploaded batch in `mode` (async on st).
 int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_bin, double w_det,
-               const double* theta_inv, uint32_t score_mask, cudaStream_t st) {
+               const double* theta_inv, uint32_t score_mask, cudaStream_t st,
+               double* moments = nullptr) {
   if (e->n_events == 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "no events uploaded");
   // Gensteps always run batched: each lane reads its genstep's record at emission.
   const int batch = (e->n_events > 1 || e->gensteps) ? (e->uniform ? kBatchUniform : kBatch) : kSingle;
   int grid = 0;
-  OPTX_TRY(engine_grid(e, mode, batch, grid));
-  const size_t smem = wave_smem(e, mode, batch);
+  OPTX_TRY(engine_grid(e, mode, batch, grid, moments != nullptr));
+  const size_t smem = wave_smem(e, mode, batch, moments != nullptr);
   const int math = e->cfg.math;
   if (e->cfg.use_graph >= 0) {
     optx_engine::Graph* g = nullptr;
-    OPTX_TRY(engine_graph(e, mode, batch, grid, &g));
+    OPTX_TRY(engine_graph(e, mode, batch, grid, &g, moments != nullptr));
     OPTX_TRY(engine_upload_args(e, mode, batch, grid, g->handle, rec, w_bin, w_det, theta_inv,
-                                score_mask, st));
+                                score_mask, st, moments));
     OPTX_CUDA(cudaEventRecord(e->ev0, st));
     OPTX_CUDA(cudaGraphLaunch(g->exec, st));
     OPTX_CUDA(cudaEventRecord(e->ev1, st));
   } else {
     OPTX_TRY(engine_upload_args(e, mode, batch, grid, 0ull, rec, w_bin, w_det, theta_inv,
-                                score_mask, st));
+                                score_mask, st, moments));
     OPTX_CUDA(cudaEventRecord(e->ev0, st));
     OPTX_CUDA(DISPATCH(math, launch_wave_prep, e->d_args, e->d_ctrl,
                        std::max(1, std::min(grid, 4 * e->n_sm)), 256, st));
@@ -1282,17 +1289,17 @@ int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* s
                     static_cast<cudaStream_t>(stream));
 }
 
-int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_det,
-                            double* dev_grad, void* stream) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (e == nullptr || dev_w_bin == nullptr || dev_grad == nullptr)
-    return fail(OPTX_ERR_INVALID_ARGUMENT, "engine, dev_w_bin and dev_grad must not be NULL");
+namespace {
+
+// Score coefficients of the uploaded single configuration, theta = (abs_length,
+// scat_length, reflectivity, tau): inv = (1/La, 1/La^2, 1/Ls, 1/Ls^2, 1/R, 1/tau,
+// 1/tau^2) and the mask of parameters whose process is on.
+int adjoint_setup(optx_engine* e, double inv[7], uint32_t& mask) {
   if (e->n_tallies != 1)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "the adjoint runs on a single-configuration batch");
   const DevParams& P = e->h_params[0];
-  // theta = (abs_length, scat_length, reflectivity, tau) of the uploaded configuration.
   const double la = P.abs_length, ls = P.scat_length, R = P.refl0, tau = P.tau;
-  uint32_t mask = 0;
+  mask = 0;
   if (std::isfinite(la)) mask |= 1u;
   if (std::isfinite(ls)) mask |= 2u;
   bool painted = false;
@@ -1302,13 +1309,43 @@ int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_de
   }
   if (painted && R > 0.0) mask |= 4u;
   if (tau > 0.0) mask |= 8u;
-  const double inv[7] = {1.0 / la, 1.0 / (la * la), 1.0 / ls, 1.0 / (ls * ls),
-                         R > 0.0 ? 1.0 / R : 0.0, tau > 0.0 ? 1.0 / tau : 0.0,
-                         tau > 0.0 ? 1.0 / (tau * tau) : 0.0};
+  inv[0] = 1.0 / la;
+  inv[1] = 1.0 / (la * la);
+  inv[2] = 1.0 / ls;
+  inv[3] = 1.0 / (ls * ls);
+  inv[4] = R > 0.0 ? 1.0 / R : 0.0;
+  inv[5] = tau > 0.0 ? 1.0 / tau : 0.0;
+  inv[6] = tau > 0.0 ? 1.0 / (tau * tau) : 0.0;
+  return OPTX_OK;
+}
+
+}  // namespace
+
+int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_det,
+                            double* dev_grad, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr || dev_w_bin == nullptr || dev_grad == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "engine, dev_w_bin and dev_grad must not be NULL");
+  double inv[7];
+  uint32_t mask = 0;
+  OPTX_TRY(adjoint_setup(e, inv, mask));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   OPTX_TRY(engine_run(e, kModeAdjoint, nullptr, dev_w_bin, w_det, inv, mask, st));
   OPTX_CUDA(cudaMemcpyAsync(dev_grad, e->d_grad, 4 * sizeof(double), cudaMemcpyDeviceToDevice, st));
   return OPTX_OK;
+}
+
+int optx_engine_run_score_moments(optx_engine* e, double* dev_moments, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr || dev_moments == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "engine and dev_moments must not be NULL");
+  if ((reinterpret_cast<uintptr_t>(dev_moments) & 7u) != 0u)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "dev_moments must be 8-byte aligned");
+  double inv[7];
+  uint32_t mask = 0;
+  OPTX_TRY(adjoint_setup(e, inv, mask));
+  return engine_run(e, kModeAdjoint, nullptr, nullptr, 0.0, inv, mask,
+                    static_cast<cudaStream_t>(stream), dev_moments);
 }
 
 int optx_engine_tally_ptr(optx_engine* e, uint64_t** dev_ptr, uint64_t* len_per_event) {

@@ -204,6 +204,11 @@ __global__ void wave_prep_kernel(const WaveArgs* __restrict__ A, WaveCtrl* __res
     ctrl->spills = 0u;
   }
   if (blockIdx.x == 0 && threadIdx.x < 4u && A->grad != nullptr) A->grad[threadIdx.x] = 0.0;
+  if (A->moments != nullptr) {
+    const uint32_t nm = 5u * (A->tc.time_bins + 1u);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nm; i += gridDim.x * blockDim.x)
+      A->moments[i] = 0.0;
+  }
   if (A->tally != nullptr) {
     const size_t total = static_cast<size_t>(A->n_tallies) * A->tc.len;
     for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
@@ -246,6 +251,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
   unsigned char* extra = smem_raw + nwarps * kPantryBytesPerWarp;
   uint32_t* s_hist = reinterpret_cast<uint32_t*>(extra);
   double* s_w = reinterpret_cast<double*>(extra);
+  double* s_mom = s_w + (A->tc.time_bins + 1u);  // adjoint, moments_smem: [time_bins + 1][5]
   unsigned long long* s_evc = reinterpret_cast<unsigned long long*>(extra) + warp * 16u;
   __shared__ double s_red[4][16];
 
@@ -309,7 +315,11 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     }
   }
   if (MODE == kModeAdjoint) {
-    for (uint32_t b = threadIdx.x; b <= tc.time_bins; b += blockDim.x) s_w[b] = A->w_bin[b];
+    const double* wb = A->w_bin;
+    for (uint32_t b = threadIdx.x; b <= tc.time_bins; b += blockDim.x) s_w[b] = wb ? wb[b] : 0.0;
+    if (A->moments_smem) {
+      for (uint32_t i = threadIdx.x; i < 5u * (tc.time_bins + 1u); i += blockDim.x) s_mom[i] = 0.0;
+    }
   }
   __syncthreads();
 
@@ -410,14 +420,28 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
       }
     } else {  // adjoint: score terms of detected photons (see WaveArgs)
       if (fate == kDetected) {
-        const double w = s_w[time_bin(s.t, tc.tscale, tc.time_bins)] + A->w_det;
-        if (w != 0.0) {
+        const uint32_t tb = time_bin(s.t, tc.tscale, tc.time_bins);
+        const double w = s_w[tb] + A->w_det;
+        double* M = A->moments;
+        if (w != 0.0 || M != nullptr) {
           const double path = s.path;
           const uint32_t m = A->score_mask;
-          if (m & 1u) g0 += w * (path * A->inv_la2);
-          if (m & 2u) g1 += w * (path * A->inv_ls2 - static_cast<double>(s.ns) * A->inv_ls);
-          if (m & 4u) g2 += w * (static_cast<double>(aux.n_refl) * A->inv_r);
-          if (m & 8u) g3 += w * (static_cast<double>(aux.t_emit) * A->inv_tau2 - A->inv_tau);
+          const double s0 = (m & 1u) ? path * A->inv_la2 : 0.0;
+          const double s1 = (m & 2u) ? path * A->inv_ls2 - static_cast<double>(s.ns) * A->inv_ls : 0.0;
+          const double s2 = (m & 4u) ? static_cast<double>(aux.n_refl) * A->inv_r : 0.0;
+          const double s3 = (m & 8u) ? static_cast<double>(aux.t_emit) * A->inv_tau2 - A->inv_tau : 0.0;
+          g0 += w * s0;
+          g1 += w * s1;
+          g2 += w * s2;
+          g3 += w * s3;
+          if (M != nullptr) {  // per-bin (count, score sums): histogram and Jacobian in one pass
+            double* mb = (A->moments_smem ? s_mom : M) + 5u * tb;
+            atomicAdd(mb, 1.0);
+            if (s0 != 0.0) atomicAdd(mb + 1, s0);
+            if (s1 != 0.0) atomicAdd(mb + 2, s1);
+            if (s2 != 0.0) atomicAdd(mb + 3, s2);
+            if (s3 != 0.0) atomicAdd(mb + 4, s3);
+          }
         }
       }
     }
@@ -663,6 +687,12 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
       double acc = 0.0;
       for (uint32_t w = 0; w < nwarps; ++w) acc += s_red[threadIdx.x][w];
       if (acc != 0.0) atomicAdd(&A->grad[threadIdx.x], acc);
+    }
+    if (A->moments_smem) {  // every lane's moments are in s_mom (barrier above)
+      double* M = A->moments;
+      for (uint32_t i = threadIdx.x; i < 5u * (tc.time_bins + 1u); i += blockDim.x) {
+        if (s_mom[i] != 0.0) atomicAdd(M + i, s_mom[i]);
+      }
     }
   }
 

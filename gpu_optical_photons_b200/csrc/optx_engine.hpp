@@ -43,8 +43,10 @@ struct WaveArgs {
   double w_det;
   double inv_la, inv_la2, inv_ls, inv_ls2, inv_r, inv_tau, inv_tau2;
   uint32_t score_mask;                  // bit j: parameter j has a score term
-  uint32_t pad;
+  uint32_t moments_smem;                // 1: moments accumulate per block in shared memory first
   double* grad;                         // adjoint mode: 4 FP64 sums (accumulated)
+  double* moments;                      // adjoint mode, optional: (time_bins + 1) x 5 FP64
+                                        // per-bin (count, sum S_La, S_Ls, S_R, S_tau)
   unsigned long long graph_handle;      // cudaGraphConditionalHandle of the wave loop
   unsigned long long iter_cap;          // watchdog: max loop iterations per warp per wave
   uint32_t use_graph;                   // 1: the wave loop is a graph while node (set its condition)
@@ -90,6 +92,14 @@ constexpr uint32_t kSlotBins = 256u;
 constexpr uint32_t kSlotCounterBytesPerWarp = 2u * 8u * 8u;
 inline __host__ __device__ uint32_t slot_bin_bytes_per_warp(uint32_t n_bins) {
   return n_bins <= kSlotBins ? 2u * n_bins * 4u : 0u;
+}
+// Score moments: a block-private (time_bins + 1) x 5 FP64 table in shared memory,
+// added to global memory once per block, when it takes at most this many bytes
+// (818 time bins); larger tables accumulate with global atomics directly.
+constexpr uint32_t kMomentSmemMaxBytes = 32u * 1024u;
+inline __host__ __device__ uint32_t moment_smem_bytes(uint32_t time_bins) {
+  const uint32_t b = (time_bins + 1u) * 5u * 8u;
+  return b <= kMomentSmemMaxBytes ? b : 0u;
 }
 
 #define OPTX_DECLARE_LAUNCHERS(NS)                                                               \

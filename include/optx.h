@@ -223,6 +223,16 @@ int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* s
  * doubles, overwritten): device pointers. Asynchronous on `stream`. */
 int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_det,
                             double* dev_grad, void* stream);
+/* Per-bin score moments (extension, same replay as optx_engine_run_adjoint):
+ * for each arrival-time bin b (time_bins + 1 entries, the last = overflow)
+ *   moments[5 b + 0] = detected photons in b  (the run's histogram h_b)
+ *   moments[5 b + 1 + j] = sum over them of S_j
+ * so that moments[5 b + 1 + j] estimates dE[h_b]/dtheta_j: the Jacobian of the
+ * histogram, from which the Poisson Fisher information and Gauss-Newton steps
+ * follow without one replay per bin. Counts are exact integers in FP64.
+ * dev_moments: device pointer, (time_bins + 1) x 5 doubles, overwritten.
+ * Asynchronous on `stream`. */
+int optx_engine_run_score_moments(optx_engine* e, double* dev_moments, void* stream);
 /* Device pointer of the per-event tallies (n_events x tally length u64). */
 int optx_engine_tally_ptr(optx_engine* e, uint64_t** dev_ptr, uint64_t* len_per_event);
 /* Copies the per-event tallies to host memory (synchronises `stream`). */

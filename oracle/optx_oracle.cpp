@@ -759,6 +759,39 @@ int oracle_adjoint(const Params* p, const TallyConfig* c, uint64_t n, uint64_t f
   return 0;
 }
 
+// Per-bin score moments: moments[5 b] = detected photons in arrival-time bin b,
+// moments[5 b + 1 + j] = sum over them of S_j (the score terms of
+// oracle_adjoint, detected photons only), b = 0 .. time_bins (last = overflow).
+int oracle_score_moments(const Params* p, const TallyConfig* c, uint64_t n, uint64_t first_id,
+                         int mode, int threads, double* moments) {
+  const Surf sf = make_surf(*p, nullptr);
+  const int64_t count = static_cast<int64_t>(n);
+  const double La = p->abs_length, Ls = p->scat_length, R = p->reflectivity, tau = p->tau;
+  const bool la_on = !std::isinf(La), ls_on = !std::isinf(Ls), tau_on = tau > 0.0;
+  const int nt = threads > 0 ? threads : omp_get_max_threads();
+  const size_t len = static_cast<size_t>(c->time_bins + 1) * 5;
+  std::vector<double> part(static_cast<size_t>(nt) * len, 0.0);
+#pragma omp parallel num_threads(nt)
+  {
+    double* m = &part[static_cast<size_t>(omp_get_thread_num()) * len];
+#pragma omp for schedule(static)
+    for (int64_t i = 0; i < count; ++i) {
+      const Result r = run_one(mode, *p, sf, first_id + static_cast<uint64_t>(i));
+      if (r.fate != Detected) continue;
+      double* mb = m + 5 * static_cast<size_t>(time_bin(r.t, *c));
+      mb[0] += 1.0;
+      if (la_on) mb[1] += r.path / (La * La);
+      if (ls_on) mb[2] += r.path / (Ls * Ls) - static_cast<double>(r.ns) / Ls;
+      mb[3] += static_cast<double>(r.ex.n_refl) / R;
+      if (tau_on) mb[4] += -1.0 / tau + static_cast<double>(r.ex.t_emit) / (tau * tau);
+    }
+  }
+  for (size_t k = 0; k < len; ++k) moments[k] = 0.0;
+  for (int t = 0; t < nt; ++t)
+    for (size_t k = 0; k < len; ++k) moments[k] += part[static_cast<size_t>(t) * len + k];
+  return 0;
+}
+
 // Algorithmic op counts per step kind, over photons first_id .. first_id+n-1
 // (single thread). counts[k*4 + {0,1,2,3}] = {steps, fp ops, transcendental, int ops}
 // for k in StepKind (kStart counts photon emissions). Philox blocks are charged

@@ -52,6 +52,7 @@ def lib():
                                          ctypes.c_int, _P] + [_P] * 8
         L.oracle_adjoint.argtypes = [_P, _P, _u64, _u64, ctypes.c_int, ctypes.c_int, _P,
                                      ctypes.c_double, _P, _P, _P]
+        L.oracle_score_moments.argtypes = [_P, _P, _u64, _u64, ctypes.c_int, ctypes.c_int, _P]
         L.oracle_opcount.argtypes = [_P, _P, _u64, _u64, _P]
         L.oracle_stream.argtypes = [_u64, _u64, ctypes.c_uint32, ctypes.c_uint32, _P]
         L.oracle_philox.argtypes = [_P, _P, _P]
@@ -198,6 +199,14 @@ def adjoint(p, c, n: int, w_bin=None, w_det: float = 0.0, first_id: int = 0,
     lib().oracle_adjoint(ctypes.byref(cp), ctypes.byref(cc), n, first_id, mode, threads,
                          _ptr(wb), float(w_det), _ptr(grad), _ptr(hist), _ptr(det))
     return grad, hist, int(det[0])
+
+
+def score_moments(p, c, n: int, first_id: int = 0, mode: int = PLATFORM, threads: int = 0):
+    """Per-bin (count, sum of the four scores), shape (time_bins + 1, 5) (see oracle_score_moments)."""
+    out = np.zeros((c.time_bins + 1) * 5, np.float64)
+    cp, cc = p.to_c(), c.to_c()
+    lib().oracle_score_moments(ctypes.byref(cp), ctypes.byref(cc), n, first_id, mode, threads, _ptr(out))
+    return out.reshape(-1, 5)
 
 
 STEP_KINDS = ["start", "absorb", "scatter", "readout_reflect", "detect", "polished_reflect",
