@@ -325,9 +325,15 @@ __device__ __forceinline__ void start_photon(const DevParams& P, Photon& s, Rng&
 // One step (transport.hpp:71-145). Returns true while the photon is alive;
 // otherwise `fate` is set and the photon sits at its final interaction.
 // The window is advanced only for photons that stay alive.
+// One exit: every outcome falls through to the shared tail (rotation, flip,
+// window advance). With sync_mask != 0 (the lanes of the warp that call this
+// step together) the warp reconverges before the advance, so the Philox block
+// runs once per warp step for all lanes that need one rather than once per
+// divergent group.
 template <bool AUX>
 __device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& r, uint64_t id,
-                                            uint32_t& fate, ScoreAux& aux) {
+                                            uint32_t& fate, ScoreAux& aux,
+                                            uint32_t sync_mask = 0u) {
   const float u_abs = r.uniform<0>(), u_sca = r.uniform<1>();
   const float s_abs = (P.abs_length == kInf) ? kInf : -P.abs_length * m_log(u_abs);
   const float s_sca = (P.scat_length == kInf) ? kInf : -P.scat_length * m_log(u_sca);
@@ -371,15 +377,13 @@ __device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& 
   s.t = s.t + d * P.inv_speed;
   s.path = s.path + d;
 
+  uint32_t k = 2u;           // words consumed by this step
+  bool live = true, rotate = false, flip = false;
+  float ax = s.dx, ay = s.dy, az = s.dz, ct = 0.0f, phi_u = 0.0f;
   if (absorb) {
     fate = kAbsorbedBulk;
-    return false;
-  }
-
-  uint32_t k = 2u;           // words consumed by this step
-  bool rotate = false, flip = false;
-  float ax = s.dx, ay = s.dy, az = s.dz, ct = 0.0f, phi_u = 0.0f;
-  if (scatter) {
+    live = false;
+  } else if (scatter) {
     ++s.ns;
     ct = rayleigh_cos(r.uniform<2>());
     phi_u = r.uniform<3>();
@@ -400,18 +404,17 @@ __device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& 
         flip = true;
       } else {
         fate = readout ? kDetected : kEscaped;
-        return false;
+        live = false;
       }
     } else if (model == kBlack) {
       fate = kAbsorbedSurface;
-      return false;
+      live = false;
+    } else if (!(r.uniform<2>() <= face_refl(P, face))) {
+      // Painted reflector (transport.hpp:133-144): absorbed with 1 - R.
+      fate = kAbsorbedSurface;
+      live = false;
     } else {
-      // Painted reflector (transport.hpp:133-144).
       k = 3u;
-      if (!(r.uniform<2>() <= face_refl(P, face))) {
-        fate = kAbsorbedSurface;
-        return false;
-      }
       if (AUX) ++aux.n_refl;
       if (model == kSpecular) {
         flip = true;
@@ -436,8 +439,9 @@ __device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& 
     if (axis == 1) s.dy = -s.dy;
     if (axis == 2) s.dz = -s.dz;
   }
-  r.advance(k, id, P.key_lo, P.key_hi);
-  return true;
+  if (sync_mask != 0u) __syncwarp(sync_mask);
+  if (live) r.advance(k, id, P.key_lo, P.key_hi);
+  return live;
 }
 
 // Tally binning (transport.hpp:170-181); tscale = time_bins / time_max in float.
