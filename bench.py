@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint replay / forward cost measurement")
+    ap.add_argument("--no-compaction", action="store_true",
+                    help="skip the forced-compaction leg (state-queue HBM traffic)")
     ap.add_argument("--no-other-math", action="store_true",
                     help="skip timing the same batch in the other two math modes")
     ap.add_argument("--no-history-baseline", action="store_true",
@@ -216,7 +218,9 @@ def adjoint_cost(math: str, n: int = 10_000_000, reps: int = 5) -> dict:
     setup (the Lambertian cube with Rayleigh scattering and a volume source at
     theta = (La 1000, Ls 700, R 0.95, tau 4), 1e7 photons, 500 arrival-time bins):
     median CUDA-event times of the forward tally and of the replay that
-    accumulates dLoss/dtheta."""
+    accumulates dLoss/dtheta, and of the common-random-number central finite
+    differences the adjoint replaces (two forward runs per parameter, at
+    theta_j (1 +- 1e-3), parameter upload included)."""
     import torch
     from gpu_optical_photons_b200.adjoint import ResponseModel
     from gpu_optical_photons_b200.params import TallyConfig, config2
@@ -229,18 +233,65 @@ def adjoint_cost(math: str, n: int = 10_000_000, reps: int = 5) -> dict:
         w = torch.ones(tcal.time_bins + 1, dtype=torch.float64)
         m.forward(theta)
         m.replay(theta, w, 0.5)
-        fwd, adj = [], []
+        fwd, adj, fd = [], [], []
         for _ in range(reps):
+            m._upload(theta)  # back at theta after the FD runs (outside the timed regions)
+            torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(); m.engine.run_tally(); b.record(); torch.cuda.synchronize()
             fwd.append(a.elapsed_time(b))
             a.record(); m.replay(theta, w, 0.5); b.record(); torch.cuda.synchronize()
             adj.append(a.elapsed_time(b))
+            a.record()
+            for j in range(4):
+                for sgn in (1.0, -1.0):
+                    th = list(theta)
+                    th[j] = theta[j] * (1.0 + sgn * 1e-3)
+                    m._upload(th)
+                    m.engine.run_tally()
+            b.record(); torch.cuda.synchronize()
+            fd.append(a.elapsed_time(b))
     finally:
         m.close()
-    f, r = float(np.median(fwd)), float(np.median(adj))
-    return {"forward_ms": f, "replay_ms": r, "replay_over_forward": r / f, "photons": n,
+    f, r, c = float(np.median(fwd)), float(np.median(adj)), float(np.median(fd))
+    return {"forward_ms": f, "replay_ms": r, "replay_over_forward": r / f,
+            "crn_fd_ms": c, "adjoint_over_crn_fd": (f + r) / c, "photons": n,
+            "what": "adjoint = one forward + one replay; CRN FD = 8 forward runs (2 per parameter)",
             "setup": "Lambertian cube, Rayleigh, volume source, theta=(1000, 700, 0.95, 4), 500 time bins"}
+
+
+def compaction_leg(events, counts, tc, first_id, cfg, stream, tallies, hbm_peak, reps: int = 3,
+                   cadence: int = 8) -> dict:
+    """The same batch with a forced compaction every `cadence` steps per wave (the
+    reference event kernel's k steps per launch): live photons go through the
+    state queues (64 B written + 64 B read per spill), so this leg measures the
+    queues' HBM traffic. Tallies are checked equal to the one-wave run's."""
+    import torch
+    from dataclasses import replace
+    from gpu_optical_photons_b200.wavefront import WavefrontEngine
+    n_photons = int(counts.sum())
+    e2 = WavefrontEngine(tc, len(events), n_photons, replace(cfg, cadence=cadence))
+    try:
+        sptr = stream.cuda_stream
+        e2.set_events(events, counts, first_id, stream=sptr)
+        e2.run_tally(stream=sptr)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream); e2.run_tally(stream=sptr); b.record(stream); torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        st = e2.stats(stream=sptr)
+        assert np.array_equal(e2.tallies(stream=sptr), tallies), "compacted run's tallies differ"
+    finally:
+        e2.close()
+    t = float(np.median(ms))
+    qb = QUEUE_BYTES_PER_SPILL * int(st["spills"])
+    return {"cadence": cadence, "ms_per_step": t, "value": steps_of_tallies(tallies) / (t * 1e-3),
+            "waves": int(st["launches"]), "spills": int(st["spills"]), "queue_bytes": qb,
+            "queue_gbs": qb / (t * 1e-3) / 1e9, "hbm_peak_gbs": hbm_peak,
+            "queue_frac_of_hbm": qb / (t * 1e-3) / 1e9 / hbm_peak,
+            "what": "queue bytes = 128 B per spilled photon (4 x 16 B stores + 4 x 16 B loads)"}
 
 
 def run_reference(args):
@@ -488,6 +539,9 @@ def run_optx(args):
         line["other_math_modes"] = other
     if not args.no_adjoint:
         line["adjoint"] = adjoint_cost(args.math)
+    if not args.no_compaction:
+        line["compaction_leg"] = compaction_leg(events, counts, tc, first_id, cfg, stream, tallies,
+                                                hbm_peak)
     if not args.no_history_baseline:
         hv, hms, ht = history_baseline(g, events, counts, tc, first_id, args.math, stream)
         # Same per-photon arithmetic, integer tallies: the two engines agree exactly.
