@@ -200,19 +200,18 @@ def fisher_information(hist: np.ndarray, jac: np.ndarray, theta, bins: int) -> n
     return (Jp.T / lam) @ Jp
 
 
-def parameter_errors(model: "ResponseModel", theta, n_target: int | None = None) -> np.ndarray:
-    """One-sigma statistical errors of theta fitted to a target histogram of
-    n_target photons with a model of model.n photons: the inverse Fisher
-    information of the target's Poisson counts, inflated by (1 + n_target/n)
-    for the model's own sampling noise, mapped from phi to theta."""
+def parameter_errors(model: "ResponseModel", theta) -> np.ndarray:
+    """One-sigma statistical errors of theta fitted (as `calibrate` does) to a
+    target histogram of as many photons as the model runs: covariance 2 F^-1 in
+    phi — the target's Poisson counts and the model's own sampling noise
+    contribute equally — mapped from phi to theta. Parameters whose process is
+    off (zero Fisher information) get 0."""
     hist, jac = model.score_moments(theta)
     bins = model.tally.time_bins
     F = fisher_information(hist, jac, theta, bins)
     on = np.diag(F) > 0
     cov = np.zeros((4, 4))
-    cov[np.ix_(on, on)] = np.linalg.inv(F[np.ix_(on, on)])
-    nt = model.n if n_target is None else n_target
-    cov *= 1.0 + nt / model.n
+    cov[np.ix_(on, on)] = 2.0 * np.linalg.inv(F[np.ix_(on, on)])
     return np.sqrt(np.diag(cov)) * np.abs(_dtheta_dphi(theta))
 
 

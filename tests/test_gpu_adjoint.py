@@ -188,3 +188,28 @@ def test_adam_calibration_reduces_loss(engine):
     print("adam calibration", [(np.round(t, 4).tolist(), round(l, 6)) for t, l in traj])
     assert l1 < l0
     assert abs(th[3] - THETA_T[3]) < abs(THETA0[3] - THETA_T[3]) / 2
+
+
+def test_score_moments_rejects_bad_arguments(engine):
+    import ctypes
+    from gpu_optical_photons_b200 import _lib
+    from gpu_optical_photons_b200.wavefront import WavefrontEngine
+    m = ResponseModel(BASE, 1000, TC)
+    try:
+        with pytest.raises(_lib.OptxError) as e:
+            _lib.call("optx_engine_run_score_moments", m.engine._h, None, None)
+        assert e.value.code == 1
+        buf = torch.zeros((TC.time_bins + 1) * 5 + 1, dtype=torch.float64, device="cuda")
+        with pytest.raises(_lib.OptxError):  # not 8-byte aligned
+            _lib.call("optx_engine_run_score_moments", m.engine._h,
+                      ctypes.c_void_p(buf.data_ptr() + 4), None)
+    finally:
+        m.close()
+    eng = WavefrontEngine(TC, 2, 2000)
+    try:
+        eng.set_events([BASE, BASE], [1000, 1000])
+        buf = torch.zeros((TC.time_bins + 1) * 5, dtype=torch.float64, device="cuda")
+        with pytest.raises(_lib.OptxError):  # the adjoint runs on one configuration only
+            _lib.call("optx_engine_run_score_moments", eng._h, ctypes.c_void_p(buf.data_ptr()), None)
+    finally:
+        eng.close()
