@@ -296,3 +296,45 @@ def _calibrate_fisher(model: ResponseModel, theta0, target: np.ndarray, steps: i
         d[on] = np.linalg.solve(Fa + 1e-6 * np.diag(np.diag(Fa)), g[on])
         phi = phi - np.clip(lr * d, -max_step, max_step)
     return traj
+
+
+def main(argv=None):
+    """Calibration from the command line: fits theta to a target histogram made
+    at --target with its own seed, and prints one JSON line (trajectory, estimate,
+    one-sigma errors).
+
+        python -m gpu_optical_photons_b200.adjoint --n 1e7 --steps 20
+    """
+    import argparse
+    import json
+    from .params import config2
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--n", type=float, default=1e7, help="photons per evaluation")
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--method", default="fisher", choices=["fisher", "adam"])
+    ap.add_argument("--theta0", type=float, nargs=4, default=[1000.0, 700.0, 0.95, 4.0],
+                    metavar=("LA", "LS", "R", "TAU"))
+    ap.add_argument("--target", type=float, nargs=4, default=[800.0, 600.0, 0.93, 3.5],
+                    metavar=("LA", "LS", "R", "TAU"))
+    ap.add_argument("--target-seed", type=int, default=777)
+    ap.add_argument("--time_bins", type=int, default=500)
+    ap.add_argument("--time_max", type=float, default=50.0)
+    a = ap.parse_args(argv)
+    base = config2()[0]
+    n = int(a.n)
+    tally = TallyConfig(a.time_bins, a.time_max, 1)
+    target = target_histogram(base, a.target, n, seed=a.target_seed, tally=tally)
+    model = ResponseModel(base, n, tally)
+    try:
+        traj = calibrate(base, a.theta0, target, n, steps=a.steps, model=model, method=a.method)
+        est = traj[-1][0]
+        sig = parameter_errors(model, est)
+    finally:
+        model.close()
+    print(json.dumps({"method": a.method, "photons": n, "theta_names": THETA_NAMES,
+                      "target": a.target, "estimate": est.tolist(), "sigma": sig.tolist(),
+                      "trajectory": [[t.tolist(), l] for t, l in traj]}))
+
+
+if __name__ == "__main__":
+    main()

@@ -213,3 +213,12 @@ def test_score_moments_rejects_bad_arguments(engine):
             _lib.call("optx_engine_run_score_moments", eng._h, ctypes.c_void_p(buf.data_ptr()), None)
     finally:
         eng.close()
+
+
+def test_calibration_command_line(engine, capsys):
+    import json
+    from gpu_optical_photons_b200.adjoint import main
+    main(["--n", "1e6", "--steps", "4"])
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert len(out["trajectory"]) == 4 + 2 and len(out["estimate"]) == 4 and len(out["sigma"]) == 4
+    assert out["trajectory"][-1][1] < out["trajectory"][0][1]
