@@ -868,6 +868,12 @@ int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
   return OPTX_OK;
 }
 
+// History tally grid: this many waves of resident blocks, each thread looping
+// over photons (grid-stride). Measured on B200 at 1e7 photons: 4 waves take
+// 2-4 % less time than 1 wave, and one photon per thread (as many blocks as
+// photons / block, each with its own histogram set-up and flush) 8-42 % more.
+constexpr uint64_t kHistoryGridWaves = 4;
+
 int optx_run_tally(const optx_params* p, const optx_faces* faces, const optx_tally_config* c,
                    uint64_t n, uint64_t* tally_out, int block_size, uint64_t first_id, int math,
                    optx_timing* timing) {
@@ -923,7 +929,8 @@ int optx_run_tally(const optx_params* p, const optx_faces* faces, const optx_tal
   const int bps = DISPATCH(math, history_tally_blocks_per_sm, block_size, smem);
   const uint64_t needed = (n + block_size - 1) / block_size;
   const int grid = static_cast<int>(std::max<uint64_t>(
-      1, std::min<uint64_t>(needed, static_cast<uint64_t>(std::max(bps, 1)) * num_sms())));
+      1, std::min<uint64_t>(needed, kHistoryGridWaves * static_cast<uint64_t>(std::max(bps, 1)) *
+                                        num_sms())));
   if (n / grid >= 0xffffffffull)
     return fail(OPTX_ERR_RUNTIME, "too many photons for one tally launch; split the run");
   const auto ta = std::chrono::steady_clock::now();
@@ -996,7 +1003,8 @@ int optx_tally_device(const optx_params* p, const optx_faces* faces, const optx_
   const int bps = DISPATCH(math, history_tally_blocks_per_sm, block_size, smem);
   const uint64_t needed = (n + block_size - 1) / block_size;
   const int grid = static_cast<int>(std::max<uint64_t>(
-      1, std::min<uint64_t>(needed, static_cast<uint64_t>(std::max(bps, 1)) * num_sms())));
+      1, std::min<uint64_t>(needed, kHistoryGridWaves * static_cast<uint64_t>(std::max(bps, 1)) *
+                                        num_sms())));
   if (n / grid >= 0xffffffffull)
     return fail(OPTX_ERR_RUNTIME, "too many photons for one tally launch; split the run");
   OPTX_CUDA(DISPATCH(math, launch_history_tally, P, td, first_id, n,
