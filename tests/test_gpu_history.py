@@ -35,7 +35,7 @@ def test_fast_mode_agrees_with_reference_default_build(engine, golden, name, mat
     p = params_from_meta(case["params"])
     rec, _ = engine.run_gpu_records(p, case["n"], first_id=case["first_id"], math=math_mode)
     h = compare_histories(rec, golden_records(arrays, name, "platform"))
-    # Tolerance: at most 0.1% of histories with a different discrete path (north star).
+    # Tolerance: at most 0.1% of histories with a different discrete path.
     assert h["same_discrete"] >= 0.999 * case["n"] - 1, h
 
 
