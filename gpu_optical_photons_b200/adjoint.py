@@ -77,6 +77,7 @@ class ResponseModel:
         stream = torch.cuda.current_stream().cuda_stream
         _lib.call("optx_engine_run_adjoint", self.engine._h, ctypes.c_void_p(w.data_ptr()),
                   float(w_det), ctypes.c_void_p(grad.data_ptr()), ctypes.c_void_p(stream))
+        self.engine.stats(stream)  # raises if the run ended on the watchdog or a full queue
         return grad.cpu().numpy()
 
     def score_moments(self, theta) -> tuple[np.ndarray, np.ndarray]:
@@ -90,6 +91,7 @@ class ResponseModel:
         stream = torch.cuda.current_stream().cuda_stream
         _lib.call("optx_engine_run_score_moments", self.engine._h, ctypes.c_void_p(m.data_ptr()),
                   ctypes.c_void_p(stream))
+        self.engine.stats(stream)  # raises if the run ended on the watchdog or a full queue
         M = m.view(tb + 1, 5).cpu().numpy()
         return M[:, 0].copy(), M[:, 1:].copy()
 

@@ -220,7 +220,9 @@ int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* s
  * (terms of a disabled process are 0). With w_bin = dLoss/dh (h = the run's
  * arrival-time histogram, time_bins + 1 entries) and w_det = dLoss/dD / n
  * (D = detected fraction), grad = dLoss/dtheta. dev_w_bin, dev_grad (4
- * doubles, overwritten): device pointers. Asynchronous on `stream`. */
+ * doubles, overwritten): device pointers. Asynchronous on `stream`; a run that
+ * ends on the watchdog or a full state queue is reported by the next
+ * optx_engine_stats / optx_engine_get_tallies on the engine. */
 int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_det,
                             double* dev_grad, void* stream);
 /* Per-bin score moments (extension, same replay as optx_engine_run_adjoint):
@@ -231,7 +233,8 @@ int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_de
  * histogram, from which the Poisson Fisher information and Gauss-Newton steps
  * follow without one replay per bin. Counts are exact integers in FP64.
  * dev_moments: device pointer, (time_bins + 1) x 5 doubles, overwritten.
- * Asynchronous on `stream`. */
+ * Asynchronous on `stream`; run errors are reported as for
+ * optx_engine_run_adjoint. */
 int optx_engine_run_score_moments(optx_engine* e, double* dev_moments, void* stream);
 /* Device pointer of the per-event tallies (n_events x tally length u64). */
 int optx_engine_tally_ptr(optx_engine* e, uint64_t** dev_ptr, uint64_t* len_per_event);

@@ -66,3 +66,26 @@ def test_invalid_parameters_rejected_before_launch(engine):
     # and the device keeps working
     _, flat, _ = engine.run_gpu_tally(P.SimParams(), P.TallyConfig(), 1000)
     assert flat[:5].sum() == 1000
+
+
+def test_watchdog_in_adjoint_and_score_moment_runs_is_reported(engine, monkeypatch):
+    """The replay paths check the run's error word too: a watchdog stop raises
+    instead of returning a partial gradient or Jacobian."""
+    import torch
+    from gpu_optical_photons_b200.adjoint import ResponseModel
+    theta = (1000.0, 700.0, 0.95, 4.0)
+    tc = P.TallyConfig(500, 50.0, 1)
+    m = ResponseModel(P.config2()[0], 200_000, tc, config=WaveConfig(cadence=2))  # many waves
+    try:
+        w = torch.ones(tc.time_bins + 1, dtype=torch.float64)
+        monkeypatch.setenv("OPTX_TEST_FAULT", "watchdog")
+        for run in (lambda: m.replay(theta, w, 0.5), lambda: m.score_moments(theta)):
+            with pytest.raises(OptxError) as e:
+                run()
+            assert e.value.code == OPTX_ERR_WATCHDOG
+        monkeypatch.delenv("OPTX_TEST_FAULT")
+        g = m.replay(theta, w, 0.5)   # the next runs complete
+        h, _ = m.score_moments(theta)
+        assert np.all(np.isfinite(g)) and h.sum() > 0
+    finally:
+        m.close()
