@@ -68,9 +68,9 @@ constexpr float kSpeedOfLight = 299.792458f;  // mm/ns (hd.hpp:37 of the referen
 
 // Host-side fault injection for tests (unset in normal use). OPTX_TEST_FAULT=alloc
 // makes the engine's device allocations fail as cudaMalloc does when the device
-// is out of memory; OPTX_TEST_FAULT=watchdog caps every wavefront run at one wave,
-// so a run that needs more waves ends through the device-side watchdog (the
-// error word of the control block) instead of finishing.
+// is out of memory; OPTX_TEST_FAULT=watchdog caps every wavefront run at one wave
+// and each warp at one loop iteration, so a run ends through the device-side
+// watchdogs (the error word of the control block) instead of finishing.
 bool test_fault(const char* what) {
   const char* v = std::getenv("OPTX_TEST_FAULT");
   return v != nullptr && std::strcmp(v, what) == 0;
@@ -421,7 +421,10 @@ int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphC
   const unsigned long long cap =
       4ull * (max_steps + 2ull) + 4ull * (e->total / per_wave) + 64ull;
   a.wave_cap = static_cast<uint32_t>(std::min<unsigned long long>(std::max(cap, 100000ull), 0xfffffff0ull));
-  if (test_fault("watchdog")) a.wave_cap = 1u;
+  if (test_fault("watchdog")) {  // both watchdogs fire: one wave, one loop iteration per warp
+    a.wave_cap = 1u;
+    a.iter_cap = 1ull;
+  }
   a.use_graph = (e->cfg.use_graph >= 0) ? 1u : 0u;
   a.chunk = e->cfg.chunk;
   a.tail_steps = e->cfg.tail_steps;
@@ -540,12 +543,17 @@ int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_
   return OPTX_OK;
 }
 
+// Status of a finished run from its control block's error word.
+int run_error(unsigned error) {
+  if (error & kErrQueue) return fail(OPTX_ERR_CAPACITY, "wavefront state queue overflow");
+  if (error & kErrWatchdog) return fail(OPTX_ERR_WATCHDOG, "wavefront iteration cap reached");
+  return OPTX_OK;
+}
+
 int engine_check_ctrl(optx_engine* e, WaveCtrl& c, cudaStream_t st) {
   OPTX_CUDA(cudaMemcpyAsync(&c, e->d_ctrl, sizeof(c), cudaMemcpyDeviceToHost, st));
   OPTX_CUDA(cudaStreamSynchronize(st));
-  if (c.error & kErrQueue) return fail(OPTX_ERR_CAPACITY, "wavefront state queue overflow");
-  if (c.error & kErrWatchdog) return fail(OPTX_ERR_WATCHDOG, "wavefront iteration cap reached");
-  return OPTX_OK;
+  return run_error(c.error);
 }
 
 }  // namespace
@@ -564,6 +572,7 @@ struct RecPipe {
   unsigned char* pin[2] = {nullptr, nullptr};
   cudaStream_t comp = nullptr, copy = nullptr;
   cudaEvent_t k0[2], k1[2], c1[2];
+  unsigned* err = nullptr;  // pinned: the engine run's error word per buffer set
   bool events = false;
 };
 RecPipe g_pipe;
@@ -591,6 +600,8 @@ int pipe_ensure(uint64_t cap) {
       OPTX_CUDA(cudaEventCreate(&g_pipe.k1[b]));
       OPTX_CUDA(cudaEventCreate(&g_pipe.c1[b]));
     }
+    OPTX_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&g_pipe.err), 2 * sizeof(unsigned),
+                            cudaHostAllocDefault));
     g_pipe.events = true;
   }
   if (g_pipe.cap >= cap) return OPTX_OK;
@@ -888,6 +899,8 @@ int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
       const optx_records dr{d.fate, d.n_boundary, d.n_scatter, d.t, d.x, d.y, d.z, d.path};
       OPTX_TRY(optx_engine_set_events(ae->e, p, faces, &cnt, 1, first_id + done, g_pipe.comp));
       OPTX_TRY(optx_engine_run_records(ae->e, &dr, g_pipe.comp));
+      OPTX_CUDA(cudaMemcpyAsync(&g_pipe.err[b], &ae->e->d_ctrl->error, sizeof(unsigned),
+                                cudaMemcpyDeviceToHost, g_pipe.comp));
     } else {
       OPTX_CUDA(DISPATCH(math, launch_history_records, P, first_id + done, m, d, block_size, g_pipe.comp));
     }
@@ -913,6 +926,7 @@ int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
       kms += ms;
       OPTX_CUDA(cudaEventElapsedTime(&ms, g_pipe.k1[pb], g_pipe.c1[pb]));
       cms += ms;
+      if (ae != nullptr) OPTX_TRY(run_error(g_pipe.err[pb]));
       if (!direct) host_fill(i - 1);
     }
   }
@@ -923,6 +937,7 @@ int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
   kms += ms;
   OPTX_CUDA(cudaEventElapsedTime(&ms, g_pipe.k1[lb], g_pipe.c1[lb]));
   cms += ms;
+  if (ae != nullptr) OPTX_TRY(run_error(g_pipe.err[lb]));
   if (!direct) host_fill(chunks - 1);
   tm.kernel_ms = kms;
   tm.d2h_ms = cms;  // kernel end to copy end per chunk (copies overlap later kernels)

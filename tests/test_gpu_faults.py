@@ -89,3 +89,17 @@ def test_watchdog_in_adjoint_and_score_moment_runs_is_reported(engine, monkeypat
         assert np.all(np.isfinite(g)) and h.sum() > 0
     finally:
         m.close()
+
+
+def test_watchdog_in_records_host_call_is_reported(engine, monkeypatch):
+    p = P.config2()[0]
+    n = 300_000
+    monkeypatch.setenv("OPTX_TEST_FAULT", "watchdog")
+    with pytest.raises(OptxError) as e:
+        engine.run_gpu_records(p, n)
+    assert e.value.code == OPTX_ERR_WATCHDOG
+    monkeypatch.delenv("OPTX_TEST_FAULT")
+    rec, _ = engine.run_gpu_records(p, n, math="exact")  # the same call completes afterwards
+    ref = engine.records_to_numpy(engine.records_device(p, n, math="exact"))
+    for k in ("fate", "n_boundary", "n_scatter", "t", "path"):
+        assert np.array_equal(rec[k], ref[k]), k
