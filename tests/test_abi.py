@@ -88,3 +88,56 @@ def test_no_silent_cpu_fallback_without_gpu(lib):
     assert ei.value.code == 4
     with pytest.raises(g.OptxError):
         g.WavefrontEngine(P.TallyConfig())
+
+
+C_PROGRAM = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "optx.h"
+/* the layouts the ctypes binding and the reference's SimParams rely on */
+typedef char check_params[sizeof(optx_params) == 72 && offsetof(optx_params, seed) == 64 ? 1 : -1];
+typedef char check_tally[sizeof(optx_tally_config) == 12 ? 1 : -1];
+typedef char check_faces[sizeof(optx_faces) == 48 ? 1 : -1];
+typedef char check_records[sizeof(optx_records) == 64 ? 1 : -1];
+typedef char check_timing[sizeof(optx_timing) == 40 ? 1 : -1];
+typedef char check_stats[sizeof(optx_event_stats) == 40 ? 1 : -1];
+typedef char check_wave[sizeof(optx_wave_config) == 48 ? 1 : -1];
+typedef char check_genstep[sizeof(optx_genstep) == 40 ? 1 : -1];
+int main(void) {
+  optx_params p = {0};
+  int rc;
+  if (optx_abi_version() != OPTX_ABI_VERSION) return 1;
+  /* an invalid call is rejected on the host with a message, GPU or not */
+  rc = optx_run_tally(&p, NULL, NULL, 10, NULL, 256, 0, OPTX_MATH_FAST, NULL);
+  if (rc != OPTX_ERR_INVALID_ARGUMENT) return 2;
+  if (optx_last_error() == NULL || optx_last_error()[0] == 0) return 3;
+  printf("%d %d\n", optx_gpu_available(), rc);
+  return 0;
+}
+"""
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    """optx.h compiles as C99 (warnings as errors) and as C++11, and a C program
+    linked against liboptx.so runs without a GPU (host-side checks only)."""
+    import os
+    import shutil
+    cc = shutil.which("gcc") or shutil.which("cc")
+    cxx = shutil.which("g++")
+    if cc is None:
+        pytest.skip("no C compiler")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    src = tmp_path / "use_optx.c"
+    src.write_text(C_PROGRAM)
+    exe = tmp_path / "use_optx"
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", inc, str(src),
+                    "-o", str(exe), "-L", libdir, "-loptx", f"-Wl,-rpath,{libdir}"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
+    assert out.stdout.split()[1] == "1"
+    if cxx is not None:
+        cpp = tmp_path / "use_optx.cpp"
+        cpp.write_text(C_PROGRAM.replace("{0}", "{}"))
+        subprocess.run([cxx, "-std=c++11", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-I", inc,
+                        str(cpp)], check=True)
