@@ -709,7 +709,7 @@ class PageToucher {
 // ---- engines behind the reference-API host calls ------------------------------
 // optx_run_tally and optx_run_records run the wavefront engine: the same
 // per-photon arithmetic as the history kernels (bit-identical records, equal
-// integer tallies) at 1.4-2x their speed on one configuration. One engine per
+// integer tallies) at 2-4x their speed on one configuration. One engine per
 // (device, math mode, tally configuration, photon capacity) is created on first
 // use; the most recent kApiMaxEngines are kept (until optx_release_cache). A call
 // holds a reference to its engine, so an engine dropped from the cache lives until
