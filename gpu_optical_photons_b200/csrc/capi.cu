@@ -816,6 +816,23 @@ const char* optx_last_error(void) { return g_err.c_str(); }
 int optx_release_cache(void) {
   std::vector<std::shared_ptr<ApiEngine>> engines;  // destroyed after g_mu, once unused
   {
+    // The records pipeline: no records call is in flight once g_pipe_mu is held;
+    // copies left queued by a call that returned an error are drained first.
+    std::lock_guard<std::mutex> plk(g_pipe_mu);
+    if (g_pipe.events) {
+      cudaStreamSynchronize(g_pipe.comp);
+      cudaStreamSynchronize(g_pipe.copy);
+    }
+    for (int b = 0; b < 2; ++b) {
+      if (g_pipe.dev[b]) cudaFree(g_pipe.dev[b]);
+      if (g_pipe.pin[b]) cudaFreeHost(g_pipe.pin[b]);
+      g_pipe.dev[b] = nullptr;
+      g_pipe.pin[b] = nullptr;
+    }
+    g_pipe.cap = 0;
+    cudaGetLastError();  // release reports nothing; a stale error must not reach the next call
+  }
+  {
     std::lock_guard<std::mutex> lk(g_mu);
     if (g_cache.rec) cudaFree(g_cache.rec);
     if (g_cache.tally) cudaFree(g_cache.tally);

@@ -218,9 +218,12 @@ def test_host_call_engine_cache_eviction(engine):
         dev = engine.tally_device(p, c, 50_000, first_id=i)
         assert np.array_equal(flat, dev.cpu().numpy().astype(np.uint64)), i
     from gpu_optical_photons_b200 import _lib
-    assert _lib.lib().optx_release_cache() == 0
+    before, _ = engine.run_gpu_records(p, 20_000, first_id=5)
+    assert _lib.lib().optx_release_cache() == 0   # engines, staging and pipeline buffers
     _, flat, _ = engine.run_gpu_tally(p, P.TallyConfig(), 10_000)  # a fresh engine after release
     assert flat[:5].sum() == 10_000
+    after, _ = engine.run_gpu_records(p, 20_000, first_id=5)  # re-created pipeline buffers
+    assert compare_histories(after, before)["bitwise_identical"] == 20_000
 
 
 def test_host_calls_from_several_threads(engine):
