@@ -296,7 +296,6 @@ struct optx_engine {
   float4* d_qb = nullptr;
   unsigned long long* d_tally = nullptr;
   double* d_grad = nullptr;
-  double* d_wbin = nullptr;
   // current batch: n_events records (events or gensteps) adding to n_tallies slices
   uint32_t n_events = 0;
   uint32_t n_tallies = 0;
@@ -1194,8 +1193,7 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
       (rc = alloc(reinterpret_cast<void**>(&e->d_qa), qcap * 64ull)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_qb), qcap * 64ull)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_tally), 8ull * td.len * max_events)) ||
-      (rc = alloc(reinterpret_cast<void**>(&e->d_grad), 8ull * 4)) ||
-      (rc = alloc(reinterpret_cast<void**>(&e->d_wbin), 8ull * (td.time_bins + 1ull))))
+      (rc = alloc(reinterpret_cast<void**>(&e->d_grad), 8ull * 4)))
     return cleanup(rc);
   if (cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess)
     return cleanup(fail(OPTX_ERR_CUDA, "cudaEventCreate failed"));
@@ -1221,7 +1219,6 @@ int optx_engine_destroy(optx_engine* e) {
   cudaFree(e->d_qb);
   cudaFree(e->d_tally);
   cudaFree(e->d_grad);
-  cudaFree(e->d_wbin);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
   delete e;
@@ -1270,18 +1267,22 @@ int optx_engine_set_events(optx_engine* e, const optx_params* events, const optx
     return fail(OPTX_ERR_INVALID_ARGUMENT, "n_events must be in [1, max_events]");
   if (events == nullptr || counts == nullptr)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "events and counts must not be NULL");
-  e->h_params.resize(n_events);
-  e->h_offsets.resize(n_events + 1ull);
+  // Built aside and committed only when every event is valid: a rejected batch
+  // leaves the engine's current batch as it was.
+  std::vector<DevParams> hp(n_events);
+  std::vector<unsigned long long> ho(n_events + 1ull);
   uint64_t total = 0;
   for (uint32_t i = 0; i < n_events; ++i) {
     OPTX_TRY(check_params(&events[i], faces ? &faces[i] : nullptr));
-    e->h_params[i] = make_dev_params(events[i], faces ? &faces[i] : nullptr);
-    e->h_offsets[i] = total;
+    hp[i] = make_dev_params(events[i], faces ? &faces[i] : nullptr);
+    ho[i] = total;
     total += counts[i];
     if (total > e->max_photons)
       return fail(OPTX_ERR_INVALID_ARGUMENT, "batch exceeds the engine's max_photons");
   }
-  e->h_offsets[n_events] = total;
+  ho[n_events] = total;
+  e->h_params.swap(hp);
+  e->h_offsets.swap(ho);
   e->n_events = n_events;
   e->n_tallies = n_events;
   e->gensteps = false;
@@ -1311,8 +1312,8 @@ int optx_engine_set_gensteps(optx_engine* e, const optx_params* events, const op
     OPTX_TRY(check_params(&events[i], faces ? &faces[i] : nullptr));
     ev[i] = make_dev_params(events[i], faces ? &faces[i] : nullptr);
   }
-  e->h_params.resize(n_gensteps);
-  e->h_offsets.resize(n_gensteps + 1ull);
+  std::vector<DevParams> hp(n_gensteps);  // committed only when every genstep is valid
+  std::vector<unsigned long long> ho(n_gensteps + 1ull);
   std::vector<float4> seg(2ull * n_gensteps);
   std::vector<uint32_t> tally_of(n_gensteps);
   uint64_t total = 0;
@@ -1328,16 +1329,18 @@ int optx_engine_set_gensteps(optx_engine* e, const optx_params* events, const op
     d.src_x = gs.x0;
     d.src_y = gs.y0;
     d.src_z = gs.z0;
-    e->h_params[g] = d;
+    hp[g] = d;
     seg[2ull * g] = make_float4(gs.x1, gs.y1, gs.z1, gs.t0);
     seg[2ull * g + 1] = make_float4(gs.t1 - gs.t0, 0.0f, 0.0f, 0.0f);
     tally_of[g] = gs.event;
-    e->h_offsets[g] = total;
+    ho[g] = total;
     total += gs.n_photons;
     if (total > e->max_photons)
       return fail(OPTX_ERR_INVALID_ARGUMENT, "gensteps exceed the engine's max_photons");
   }
-  e->h_offsets[n_gensteps] = total;
+  ho[n_gensteps] = total;
+  e->h_params.swap(hp);
+  e->h_offsets.swap(ho);
   e->n_events = n_gensteps;
   e->n_tallies = n_events;
   e->gensteps = true;

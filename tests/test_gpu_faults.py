@@ -103,3 +103,22 @@ def test_watchdog_in_records_host_call_is_reported(engine, monkeypatch):
     ref = engine.records_to_numpy(engine.records_device(p, n, math="exact"))
     for k in ("fate", "n_boundary", "n_scatter", "t", "path"):
         assert np.array_equal(rec[k], ref[k]), k
+
+
+def test_rejected_batch_leaves_the_current_batch_intact(engine):
+    """A set_events call that fails on its third event changes nothing: the
+    engine still runs the batch uploaded before it."""
+    tc = P.TallyConfig(100, 50.0, 10)
+    good = [P.config2()[0].replace(abs_length=500.0 + 100.0 * i, max_steps=50 + i) for i in range(4)]
+    eng = WavefrontEngine(tc, 4, 40_000)
+    try:
+        eng.set_events(good, [10_000] * 4)
+        eng.run_tally()
+        before = eng.tallies()
+        bad = [good[3], good[2], P.config2()[0].replace(hx=-1.0), good[0]]
+        with pytest.raises(InvalidArgument):
+            eng.set_events(bad, [10_000] * 4)
+        eng.run_tally()
+        assert np.array_equal(eng.tallies(), before)
+    finally:
+        eng.close()
