@@ -191,6 +191,10 @@ int num_sms() {
                                 : fast::fn(__VA_ARGS__))
 
 // ---- cached device buffers (per process; the library serialises calls) ---------
+// g_cache.rec belongs to optx_run_records_event, which holds g_event_mu for its
+// whole call (its engine writes the buffer between its own g_mu sections).
+// Lock order: g_event_mu, g_pipe_mu, an API engine's mu, g_mu.
+std::mutex g_event_mu;
 struct Cache {
   void* rec = nullptr;
   size_t rec_bytes = 0;
@@ -713,7 +717,7 @@ class PageToucher {
 // use; the most recent kApiMaxEngines are kept (until optx_release_cache). A call
 // holds a reference to its engine, so an engine dropped from the cache lives until
 // its last call ends; its mutex serialises a call's upload / run / read-back
-// sequence. Lock order: g_pipe_mu, then an engine's mu, then g_mu (taken inside
+// sequence. Lock order: g_event_mu, g_pipe_mu, then an engine's mu, then g_mu (taken inside
 // the optx_engine_* calls).
 struct ApiEngine {
   int device = -1;
@@ -813,10 +817,12 @@ int optx_gpu_device_name(char* buf, size_t len) {
 const char* optx_last_error(void) { return g_err.c_str(); }
 
 int optx_release_cache(void) {
+  // No records call is in flight while g_event_mu (held to the end, so that
+  // g_cache.rec is not in use when it is freed) and g_pipe_mu are held.
+  std::lock_guard<std::mutex> elk(g_event_mu);
   std::vector<std::shared_ptr<ApiEngine>> engines;  // destroyed after g_mu, once unused
   {
-    // The records pipeline: no records call is in flight once g_pipe_mu is held;
-    // copies left queued by a call that returned an error are drained first.
+    // Copies left queued by a records call that returned an error are drained first.
     std::lock_guard<std::mutex> plk(g_pipe_mu);
     if (g_pipe.events) {
       cudaStreamSynchronize(g_pipe.comp);
@@ -1521,6 +1527,7 @@ int optx_run_records_event(const optx_params* p, const optx_faces* faces, uint64
   OPTX_TRY(check_math(math));
   if (n > 0) OPTX_TRY(check_records(out));
   OPTX_TRY(ensure_device());
+  std::lock_guard<std::mutex> event_lk(g_event_mu);  // g_cache.rec is in use until the end
   const auto t0 = std::chrono::steady_clock::now();
   const uint64_t cap = std::max<uint64_t>(1, std::min<uint64_t>({n, chunk ? chunk : (uint64_t{1} << 24), uint64_t{1} << 31}));
   optx_tally_config tc{1u, 1.0f, 1u};

@@ -244,3 +244,25 @@ def test_host_calls_from_several_threads(engine):
     with ThreadPoolExecutor(4) as pool:
         parallel = list(pool.map(job, range(12)))
     assert serial == parallel
+
+
+def test_event_records_and_cache_release_from_several_threads(engine):
+    """Event-kernel records calls of growing sizes (so the cached device buffer
+    is re-allocated) interleaved with cache releases on four threads give the
+    results of the same calls made one at a time."""
+    from concurrent.futures import ThreadPoolExecutor
+    from gpu_optical_photons_b200 import _lib
+    p = P.config2()[0]
+
+    def job(i):
+        if i % 4 == 3:
+            assert _lib.lib().optx_release_cache() == 0
+            return ("release", i)
+        n = 20_000 + 15_000 * i
+        rec, _, _ = engine.run_gpu_records_event(p, n, 4, first_id=i)
+        return ("event", i, int(rec["n_boundary"].sum()), float(rec["t"].astype(np.float64).sum()))
+
+    serial = [job(i) for i in range(12)]
+    with ThreadPoolExecutor(4) as pool:
+        parallel = list(pool.map(job, range(12)))
+    assert serial == parallel
