@@ -105,6 +105,7 @@ _SIGS = {
     "optx_engine_stats": [_P, _P, _P],
     "optx_run_batch": [_P, _P, _P, _P, ctypes.c_uint32, _u64, _P, _P, _P],
     "optx_engine_set_gensteps": [_P, _P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, _u64, _P],
+    "optx_engine_set_gensteps_device": [_P, _P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, _u64, _P],
     "optx_run_gensteps": [_P, _P, _P, ctypes.c_uint32, _P, ctypes.c_uint32, _u64, _P, _P, _P],
 }
 

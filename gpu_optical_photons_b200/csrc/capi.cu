@@ -273,6 +273,110 @@ DevRecords to_dev(const optx_records* r) {
   return {r->fate, r->n_boundary, r->n_scatter, r->t, r->x, r->y, r->z, r->path};
 }
 
+// ---- gensteps from device memory ------------------------------------------------
+// A producer on the GPU (a charged-particle step loop, say) hands its gensteps
+// over in device memory: records, segments, event indices and the photon
+// offsets are built by kernels, and the run takes its photon total from the
+// device, so nothing waits for the host. Offsets come from a two-level scan of
+// 4096-genstep tiles, hence at most 4096^2 gensteps per upload.
+constexpr uint32_t kScanBlock = 1024;                     // threads per scan block
+constexpr uint32_t kScanItems = 4;                        // gensteps per thread
+constexpr uint32_t kScanTile = kScanBlock * kScanItems;   // gensteps per scan block
+constexpr uint32_t kMaxDeviceGensteps = kScanTile * kScanTile;
+
+// One thread per genstep: its parameter record (its event's physics, source =
+// the segment from (x0, y0, z0)), segment entry, event index and photon count
+// (the scan's input), with the checks of optx_engine_set_gensteps. An invalid
+// genstep sets bit 0 of *error, adds no photons and points at event 0.
+__global__ void genstep_records_kernel(const optx_genstep* __restrict__ gs, uint32_t n,
+                                       const DevParams* __restrict__ phys, uint32_t n_events,
+                                       DevParams* __restrict__ params, float4* __restrict__ seg,
+                                       uint32_t* __restrict__ tally_of,
+                                       unsigned long long* __restrict__ counts,
+                                       unsigned int* __restrict__ error) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const optx_genstep s = gs[g];
+  const float v[8] = {s.x0, s.y0, s.z0, s.t0, s.x1, s.y1, s.z1, s.t1};
+  bool ok = s.event < n_events && s.t1 >= s.t0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) ok = ok && isfinite(v[i]);
+  if (!ok) atomicOr(error, 1u);
+  const uint32_t ev = ok ? s.event : 0u;
+  DevParams d = phys[ev];
+  d.source = kSourceSegment;
+  d.src_x = s.x0;
+  d.src_y = s.y0;
+  d.src_z = s.z0;
+  params[g] = d;
+  seg[2ull * g] = make_float4(s.x1, s.y1, s.z1, s.t0);
+  seg[2ull * g + 1] = make_float4(s.t1 - s.t0, 0.0f, 0.0f, 0.0f);
+  tally_of[g] = ev;
+  counts[g] = ok ? s.n_photons : 0ull;
+}
+
+// Exclusive scan of v[0, n) tile by tile (kScanTile entries per block), in
+// place; each tile's sum goes to tile_sums[blockIdx.x].
+__global__ void __launch_bounds__(kScanBlock) scan_tiles_kernel(unsigned long long* __restrict__ v,
+                                                                uint32_t n,
+                                                                unsigned long long* __restrict__ tile_sums) {
+  __shared__ unsigned long long s[kScanBlock];
+  const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile + threadIdx.x * kScanItems;
+  unsigned long long x[kScanItems], t = 0ull;
+#pragma unroll
+  for (uint32_t k = 0; k < kScanItems; ++k) {
+    x[k] = base + k < n ? v[base + k] : 0ull;
+    t += x[k];
+  }
+  s[threadIdx.x] = t;
+  __syncthreads();
+  for (uint32_t off = 1; off < kScanBlock; off <<= 1) {  // inclusive scan of the thread sums
+    const unsigned long long y = threadIdx.x >= off ? s[threadIdx.x - off] : 0ull;
+    __syncthreads();
+    s[threadIdx.x] += y;
+    __syncthreads();
+  }
+  unsigned long long run = s[threadIdx.x] - t;
+#pragma unroll
+  for (uint32_t k = 0; k < kScanItems; ++k) {
+    if (base + k < n) v[base + k] = run;
+    run += x[k];
+  }
+  if (threadIdx.x == kScanBlock - 1) tile_sums[blockIdx.x] = s[threadIdx.x];
+}
+
+// Adds each tile's prefix to its entries and writes the total to v[n]; a total
+// above max_total sets bit 1 of *error and becomes 0 (the run then does nothing).
+__global__ void scan_add_kernel(unsigned long long* __restrict__ v, uint32_t n,
+                                const unsigned long long* __restrict__ tile_prefix,
+                                const unsigned long long* __restrict__ grand, unsigned long long max_total,
+                                unsigned int* __restrict__ error) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) v[i] += tile_prefix[i / kScanTile];
+  if (i == 0) {
+    const unsigned long long total = *grand;
+    const bool over = total > max_total;
+    if (over) atomicOr(error, 2u);
+    v[n] = over ? 0ull : total;
+  }
+}
+
+// Photon -> record table with the total read from the device (offsets[n_records]).
+__global__ void event_table_dev_kernel(const unsigned long long* __restrict__ offsets, uint32_t n_records,
+                                       uint32_t* __restrict__ table, uint32_t shift,
+                                       unsigned long long entries) {
+  const unsigned long long k = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= entries) return;
+  const unsigned long long g = k << shift;
+  if (g >= offsets[n_records]) return;
+  uint32_t lo = 0, hi = n_records;
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (offsets[mid] <= g) lo = mid; else hi = mid;
+  }
+  table[k] = lo;
+}
+
 }  // namespace
 
 // =============================================================================
@@ -296,6 +400,7 @@ struct optx_engine {
   uint32_t* d_tally_of = nullptr;  // genstep -> event (gensteps only)
   DevParams* d_phys = nullptr;     // physics per event (gensteps only)
   float4* d_seg = nullptr;         // genstep segment ends and time windows
+  unsigned long long* d_scan = nullptr;  // device genstep uploads: tile sums of the photon scan
   float4* d_qa = nullptr;
   float4* d_qb = nullptr;
   unsigned long long* d_tally = nullptr;
@@ -306,7 +411,8 @@ struct optx_engine {
   uint32_t ev_shift = kEvShift;
   bool gensteps = false;
   bool uniform = false;  // every event has the same step physics (see same_step_physics)
-  uint64_t total = 0;
+  uint64_t total = 0;              // photons of the batch (device gensteps: the capacity bound)
+  bool total_on_device = false;    // device gensteps: the run takes its total from d_offsets[n]
   uint64_t first_id = 0;
   DevParams P0{};
   std::vector<DevParams> h_params;
@@ -505,6 +611,15 @@ int engine_graph(optx_engine* e, int mode, int batch, int grid, optx_engine::Gra
   return OPTX_OK;
 }
 
+// Device genstep uploads: the run's photon total is the scan's last entry,
+// copied device to device behind the run arguments (no host synchronisation).
+int engine_device_total(optx_engine* e, cudaStream_t st) {
+  if (e->total_on_device)
+    OPTX_CUDA(cudaMemcpyAsync(&e->d_args->total, e->d_offsets + e->n_events, sizeof(unsigned long long),
+                              cudaMemcpyDeviceToDevice, st));
+  return OPTX_OK;
+}
+
 // One complete run of the uploaded batch in `mode` (async on st).
 int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_bin, double w_det,
                const double* theta_inv, uint32_t score_mask, cudaStream_t st,
@@ -521,12 +636,14 @@ int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_
     OPTX_TRY(engine_graph(e, mode, batch, grid, &g, moments != nullptr));
     OPTX_TRY(engine_upload_args(e, mode, batch, grid, g->handle, rec, w_bin, w_det, theta_inv,
                                 score_mask, st, moments));
+    OPTX_TRY(engine_device_total(e, st));
     OPTX_CUDA(cudaEventRecord(e->ev0, st));
     OPTX_CUDA(cudaGraphLaunch(g->exec, st));
     OPTX_CUDA(cudaEventRecord(e->ev1, st));
   } else {
     OPTX_TRY(engine_upload_args(e, mode, batch, grid, 0ull, rec, w_bin, w_det, theta_inv,
                                 score_mask, st, moments));
+    OPTX_TRY(engine_device_total(e, st));
     OPTX_CUDA(cudaEventRecord(e->ev0, st));
     OPTX_CUDA(DISPATCH(math, launch_wave_prep, e->d_args, e->d_ctrl,
                        std::max(1, std::min(grid, 4 * e->n_sm)), 256, st));
@@ -556,6 +673,11 @@ int run_error(unsigned error) {
 int engine_check_ctrl(optx_engine* e, WaveCtrl& c, cudaStream_t st) {
   OPTX_CUDA(cudaMemcpyAsync(&c, e->d_ctrl, sizeof(c), cudaMemcpyDeviceToHost, st));
   OPTX_CUDA(cudaStreamSynchronize(st));
+  if (c.gs_error & 1u)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "a device genstep is invalid (event index out of range, "
+                                           "non-finite coordinate or time, or t1 < t0)");
+  if (c.gs_error & 2u)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "device gensteps exceed the engine's max_photons");
   return run_error(c.error);
 }
 
@@ -1196,11 +1318,17 @@ int optx_engine_create(const optx_tally_config* c, uint32_t max_events, uint64_t
        (rc = alloc(reinterpret_cast<void**>(&e->d_seg), 32ull * k.max_gensteps))) ||
       (k.max_gensteps > 0 &&
        (rc = alloc(reinterpret_cast<void**>(&e->d_phys), sizeof(DevParams) * max_events))) ||
+      (k.max_gensteps > 0 &&
+       (rc = alloc(reinterpret_cast<void**>(&e->d_scan), 8ull * (kScanTile + 1ull)))) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_qa), qcap * 64ull)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_qb), qcap * 64ull)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_tally), 8ull * td.len * max_events)) ||
       (rc = alloc(reinterpret_cast<void**>(&e->d_grad), 8ull * 4)))
     return cleanup(rc);
+  if (cudaMemset(e->d_ctrl, 0, sizeof(WaveCtrl)) != cudaSuccess) {  // no error, no run yet
+    cudaGetLastError();
+    return cleanup(fail(OPTX_ERR_CUDA, "cudaMemset of the control block failed"));
+  }
   if (cudaEventCreate(&e->ev0) != cudaSuccess || cudaEventCreate(&e->ev1) != cudaSuccess)
     return cleanup(fail(OPTX_ERR_CUDA, "cudaEventCreate failed"));
   *out = e;
@@ -1221,6 +1349,7 @@ int optx_engine_destroy(optx_engine* e) {
   cudaFree(e->d_tally_of);
   cudaFree(e->d_seg);
   cudaFree(e->d_phys);
+  cudaFree(e->d_scan);
   cudaFree(e->d_qa);
   cudaFree(e->d_qb);
   cudaFree(e->d_tally);
@@ -1249,6 +1378,8 @@ static bool same_step_physics(DevParams a, DevParams b) {
 // photon -> record table at the finest resolution the table holds.
 static int engine_upload_records(optx_engine* e, cudaStream_t st) {
   const uint32_t n = e->n_events;
+  e->total_on_device = false;
+  OPTX_CUDA(cudaMemsetAsync(&e->d_ctrl->gs_error, 0, sizeof(unsigned), st));
   OPTX_CUDA(cudaMemcpyAsync(e->d_params, e->h_params.data(), sizeof(DevParams) * n,
                             cudaMemcpyHostToDevice, st));
   OPTX_CUDA(cudaMemcpyAsync(e->d_offsets, e->h_offsets.data(), 8ull * (n + 1ull),
@@ -1362,6 +1493,67 @@ int optx_engine_set_gensteps(optx_engine* e, const optx_params* events, const op
   OPTX_TRY(engine_upload_records(e, st));
   // The host vectors must outlive the asynchronous copies.
   OPTX_CUDA(cudaStreamSynchronize(st));
+  return OPTX_OK;
+}
+
+int optx_engine_set_gensteps_device(optx_engine* e, const optx_params* events,
+                                    const optx_faces* faces, uint32_t n_events,
+                                    const optx_genstep* dev_gensteps, uint32_t n_gensteps,
+                                    uint64_t first_id, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "engine must not be NULL");
+  if (n_events == 0 || n_events > e->max_events)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "n_events must be in [1, max_events]");
+  if (n_gensteps == 0 || n_gensteps > e->cfg.max_gensteps || n_gensteps > kMaxDeviceGensteps)
+    return fail(OPTX_ERR_INVALID_ARGUMENT,
+                "n_gensteps must be in [1, min(max_gensteps, 2^24)] for device gensteps");
+  if (events == nullptr || dev_gensteps == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "events and dev_gensteps must not be NULL");
+  if ((reinterpret_cast<uintptr_t>(dev_gensteps) & 3u) != 0u)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "dev_gensteps must be 4-byte aligned");
+  std::vector<DevParams> ev(n_events);
+  for (uint32_t i = 0; i < n_events; ++i) {
+    OPTX_TRY(check_params(&events[i], faces ? &faces[i] : nullptr));
+    ev[i] = make_dev_params(events[i], faces ? &faces[i] : nullptr);
+    ev[i].source = kSourceSegment;  // the records the device builds from them
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const uint32_t n = n_gensteps;
+  const uint32_t tiles = (n + kScanTile - 1u) / kScanTile;
+  // ev is staged by the copy before it returns (pageable host memory).
+  OPTX_CUDA(cudaMemcpyAsync(e->d_phys, ev.data(), sizeof(DevParams) * n_events, cudaMemcpyHostToDevice, st));
+  OPTX_CUDA(cudaMemsetAsync(&e->d_ctrl->gs_error, 0, sizeof(unsigned), st));
+  genstep_records_kernel<<<(n + 255u) / 256u, 256, 0, st>>>(
+      dev_gensteps, n, e->d_phys, n_events, e->d_params, e->d_seg, e->d_tally_of, e->d_offsets,
+      &e->d_ctrl->gs_error);
+  OPTX_CUDA(cudaGetLastError());
+  scan_tiles_kernel<<<tiles, kScanBlock, 0, st>>>(e->d_offsets, n, e->d_scan);
+  OPTX_CUDA(cudaGetLastError());
+  scan_tiles_kernel<<<1, kScanBlock, 0, st>>>(e->d_scan, tiles, e->d_scan + kScanTile);
+  OPTX_CUDA(cudaGetLastError());
+  scan_add_kernel<<<(n + 255u) / 256u, 256, 0, st>>>(e->d_offsets, n, e->d_scan, e->d_scan + kScanTile,
+                                                     e->max_photons, &e->d_ctrl->gs_error);
+  OPTX_CUDA(cudaGetLastError());
+  // The photon -> record table at the resolution the capacity allows.
+  uint32_t shift = 0;
+  while (shift < kEvShift && (e->max_photons >> shift) + 2ull > e->ev_entries) ++shift;
+  const unsigned long long entries = (e->max_photons >> shift) + 1ull;
+  event_table_dev_kernel<<<static_cast<unsigned>((entries + 255ull) / 256ull), 256, 0, st>>>(
+      e->d_offsets, n, e->d_evtable, shift, entries);
+  OPTX_CUDA(cudaGetLastError());
+  e->h_params.swap(ev);  // per-event physics on the host: caps and the adjoint's coefficients
+  e->h_offsets.clear();
+  e->n_events = n;
+  e->n_tallies = n_events;
+  e->gensteps = true;
+  e->uniform = true;
+  for (uint32_t i = 1; i < n_events && e->uniform; ++i)
+    e->uniform = same_step_physics(e->h_params[0], e->h_params[i]);
+  e->ev_shift = shift;
+  e->total = e->max_photons;  // bound for the watchdog caps; the run reads the real total
+  e->total_on_device = true;
+  e->first_id = first_id;
+  e->P0 = e->h_params[0];
   return OPTX_OK;
 }
 

@@ -73,6 +73,8 @@ struct WaveCtrl {
   unsigned int active;             // 0 once the run is complete
   unsigned int error;              // bit 0 queue overflow, bit 1 watchdog
   unsigned int spills;             // total photons spilled over the run
+  unsigned int gs_error;           // device genstep upload: bit 0 an invalid genstep, bit 1 more
+                                   // photons than the engine holds (kept until the next upload)
 };
 
 enum WaveMode : int { kModeTally = 0, kModeRecords = 1, kModeAdjoint = 2 };

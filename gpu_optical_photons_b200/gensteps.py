@@ -48,6 +48,14 @@ def as_gensteps(g) -> np.ndarray:
     return out
 
 
+def to_device(gensteps, device="cuda"):
+    """The gensteps as a torch uint8 tensor in device memory (40 bytes per
+    genstep, the optx_genstep layout), for WavefrontEngine.set_gensteps_device."""
+    import torch
+    g = as_gensteps(gensteps)
+    return torch.from_numpy(np.ascontiguousarray(g).view(np.uint8)).to(device)
+
+
 def photons_of(gensteps) -> int:
     return int(np.asarray(as_gensteps(gensteps)["n_photons"], dtype=np.uint64).sum())
 

@@ -106,6 +106,23 @@ class WavefrontEngine:
         self.n_events = len(events)
         self.counts = np.bincount(g["event"], weights=g["n_photons"], minlength=len(events)).astype(np.uint64)
 
+    def set_gensteps_device(self, events, dev_gensteps, first_id: int = 0, stream=0):
+        """Uploads gensteps that are already in device memory (a CUDA tensor of
+        optx_genstep records, 40 bytes each, e.g. from gensteps.to_device): the
+        records and photon offsets are built on the device, asynchronously on
+        `stream`. Invalid gensteps are reported by the next tallies() / stats()."""
+        nbytes = dev_gensteps.numel() * dev_gensteps.element_size()
+        if not dev_gensteps.is_cuda or not dev_gensteps.is_contiguous() or nbytes % 40:
+            raise ValueError("dev_gensteps must be a contiguous CUDA tensor of 40-byte gensteps")
+        arr, faces = _events_c(events)
+        self._keep = (arr, faces, dev_gensteps)
+        _lib.call("optx_engine_set_gensteps_device", self._h, ctypes.cast(arr, ctypes.c_void_p),
+                  ctypes.cast(faces, ctypes.c_void_p) if faces is not None else None, len(events),
+                  ctypes.c_void_p(dev_gensteps.data_ptr()), nbytes // 40, first_id,
+                  ctypes.c_void_p(stream or 0))
+        self.n_events = len(events)
+        self.counts = None  # known on the device only
+
     def run_gensteps(self, events, gensteps, first_id: int = 0):
         """One-shot host-buffer genstep run: upload, graph launch, D2H per-event tallies."""
         from .gensteps import as_gensteps

@@ -203,6 +203,22 @@ int optx_engine_set_events(optx_engine* e, const optx_params* events, const optx
 int optx_engine_set_gensteps(optx_engine* e, const optx_params* events, const optx_faces* faces,
                              uint32_t n_events, const optx_genstep* gensteps, uint32_t n_gensteps,
                              uint64_t first_id, void* stream);
+/* The same upload with the gensteps in device memory (extension), for a
+ * producer that runs on the GPU: kernels on `stream` build the records, segment
+ * table, event indices and photon offsets, and the next run takes its photon
+ * total from the device, so neither the upload nor the run waits for the host
+ * (the small per-event table in `events` is staged before the call returns).
+ * dev_gensteps: device pointer, 4-byte aligned, n_gensteps <= min(max_gensteps,
+ * 2^24). The gensteps are checked on the device as optx_engine_set_gensteps
+ * checks them on the host; an invalid one, or more photons than the engine
+ * holds, is reported as OPTX_ERR_INVALID_ARGUMENT by the next
+ * optx_engine_get_tallies / optx_engine_stats (the run then tallies without
+ * the invalid gensteps, or nothing when over capacity). Results equal those of
+ * optx_engine_set_gensteps with the same gensteps. */
+int optx_engine_set_gensteps_device(optx_engine* e, const optx_params* events,
+                                    const optx_faces* faces, uint32_t n_events,
+                                    const optx_genstep* dev_gensteps, uint32_t n_gensteps,
+                                    uint64_t first_id, void* stream);
 /* Runs the uploaded batch; per-event tallies stay on the device (overwritten).
  * Asynchronous on `stream`. */
 int optx_engine_run_tally(optx_engine* e, void* stream);

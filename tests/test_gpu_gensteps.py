@@ -156,3 +156,93 @@ def test_set_events_after_gensteps(engine, oracle):
     offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
     arr = (P.CSimParams * 4)(*[e.to_c() for e in evs])
     assert np.array_equal(b, oracle.batch_tally(arr, offs, TC, mode=oracle.PORTABLE))
+
+
+@pytest.mark.parametrize("cfg", [{}, {"use_graph": False, "cadence": 3}, {"math": "fast"}])
+def test_device_gensteps_equal_host_gensteps(engine, oracle, cfg):
+    """Gensteps uploaded from device memory give the host upload's tallies and
+    records, bit for bit (exact mode: the oracle's too)."""
+    import torch
+    events, g = _workload()
+    n = G.photons_of(g)
+    eng = _engine(events, g, **cfg)
+    try:
+        eng.set_gensteps(events, g, first_id=77)
+        eng.run_tally()
+        host = eng.tallies()
+        dh = engine.device_records(n)
+        eng.run_records(dh)
+        dg = G.to_device(g)
+        stream = torch.cuda.current_stream().cuda_stream
+        eng.set_gensteps_device(events, dg, first_id=77, stream=stream)
+        eng.run_tally(stream=stream)
+        dev = eng.tallies(stream=stream)
+        dd = engine.device_records(n)
+        eng.run_records(dd, stream=stream)
+        torch.cuda.synchronize()
+    finally:
+        eng.close()
+    assert np.array_equal(dev, host)
+    rh, rd = engine.records_to_numpy(dh), engine.records_to_numpy(dd)
+    assert compare_histories(rd, rh)["bitwise_identical"] == n
+    if cfg.get("math", "exact") == "exact":
+        ref, _ = oracle.genstep_run(events, g, TC, first_id=77, mode=oracle.PORTABLE)
+        assert np.array_equal(dev, ref)
+
+
+def test_device_gensteps_many_tiles(engine):
+    """More gensteps than one scan tile (4096): the two-level photon-offset scan."""
+    events, g = G.muon_events(64, seed=9, photons_per_mm=4.0, step_mm=0.25)
+    assert len(g) > 2 * 4096  # three tiles
+    eng = _engine(events, g, math="fast")
+    try:
+        eng.set_gensteps(events, g)
+        eng.run_tally()
+        host = eng.tallies()
+        eng.set_gensteps_device(events, G.to_device(g))
+        eng.run_tally()
+        assert np.array_equal(eng.tallies(), host)
+    finally:
+        eng.close()
+
+
+def test_device_genstep_errors_reported_on_the_device(engine):
+    """An invalid device genstep, or more photons than the engine holds, is
+    reported by the next tallies(); a valid upload afterwards runs normally."""
+    events, g = _workload(n_events=6)
+    eng = _engine(events, g)
+    try:
+        eng.set_gensteps(events, g)
+        eng.run_tally()
+        good = eng.tallies()
+        for bad_field, value in (("event", len(events)), ("t1", -1.0), ("x0", np.nan)):
+            b = g.copy()
+            b[bad_field][3] = value
+            eng.set_gensteps_device(events, G.to_device(b))
+            eng.run_tally()
+            with pytest.raises(InvalidArgument):
+                eng.tallies()
+        big = g.copy()
+        big["n_photons"][0] = eng.max_photons  # over the engine's capacity
+        eng.set_gensteps_device(events, G.to_device(big))
+        eng.run_tally()
+        with pytest.raises(InvalidArgument):
+            eng.tallies()
+        with pytest.raises(InvalidArgument):  # more than max_gensteps: rejected on the host
+            _lib_call_too_many(eng, events)
+        eng.set_gensteps_device(events, G.to_device(g))
+        eng.run_tally()
+        assert np.array_equal(eng.tallies(), good)
+    finally:
+        eng.close()
+
+
+def _lib_call_too_many(eng, events):
+    import ctypes
+    import torch
+    from gpu_optical_photons_b200 import _lib
+    from gpu_optical_photons_b200.wavefront import _events_c
+    arr, faces = _events_c(events)
+    dummy = torch.zeros(40, dtype=torch.uint8, device="cuda")
+    _lib.call("optx_engine_set_gensteps_device", eng._h, ctypes.cast(arr, ctypes.c_void_p), None,
+              len(events), ctypes.c_void_p(dummy.data_ptr()), eng.config.max_gensteps + 1, 0, None)
