@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint replay / forward cost measurement")
+    ap.add_argument("--no-single-configs", action="store_true",
+                    help="skip the single-configuration legs (configs 2 and 3 at 1e8 photons)")
     ap.add_argument("--no-compaction", action="store_true",
                     help="skip the forced-compaction leg (state-queue HBM traffic)")
     ap.add_argument("--no-other-math", action="store_true",
@@ -324,6 +326,55 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def single_config_legs(math: str, n: int = 100_000_000, reps: int = 3) -> dict:
+    """One configuration at its specified size (the wrapped-Lambertian cube with
+    Rayleigh scattering and the all-specular long bar, 1e8 photons each, tally
+    mode): the wavefront engine (host-call settings: 7 blocks of 128 threads),
+    this library's history kernel and, when built, the reference's tally kernel
+    on the same GPU. Median CUDA-event kernel times."""
+    import torch
+    from gpu_optical_photons_b200 import backend as B
+    from gpu_optical_photons_b200.params import config2, config3
+    from gpu_optical_photons_b200.wavefront import WaveConfig, WavefrontEngine
+
+    def ev_ms(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(); fn(); b.record(); torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts))
+
+    O = None
+    try:
+        from oracle import oracle as O
+        if not O.refgpu_available():
+            O = None
+    except Exception:
+        O = None
+    out = {}
+    for name, (p, c) in (("wrapped_lambertian_rayleigh", config2()), ("long_bar_specular", config3(False))):
+        eng = WavefrontEngine(c, 1, n, WaveConfig(blocks_per_sm=7, math=math))
+        try:
+            eng.set_events([p], [n])
+            wave = ev_ms(eng.run_tally)
+            t = eng.tallies()[0]
+        finally:
+            eng.close()
+        steps = int(t[-2] + t[-1] + t[1])
+        dev = torch.zeros(c.length, dtype=torch.int64, device="cuda")
+        hist = ev_ms(lambda: B.tally_device(p, c, n, out=dev, math=math))
+        row = {"photons": n, "photon_steps": steps, "wavefront_ms": wave, "history_ms": hist,
+               "wavefront_photon_steps_per_s": steps / (wave * 1e-3)}
+        if O is not None and math == "fast":
+            row["reference_kernel_ms"] = float(np.median([O.refgpu_tally(p, c, n)[1]["kernel_ms"]
+                                                          for _ in range(reps)]))
+        out[name] = row
+    return out
+
+
 def reference_gpu_leg(events, counts, tc):
     """The same batch through the reference's own GPU backend rebuilt for sm_100a
     (oracle/_ref/libref_gpu.so: src/gpu/gpu_backend.cu compiled by nvcc from the
@@ -539,6 +590,8 @@ def run_optx(args):
         line["other_math_modes"] = other
     if not args.no_adjoint:
         line["adjoint"] = adjoint_cost(args.math)
+    if not args.no_single_configs:
+        line["single_configs"] = single_config_legs(args.math)
     if not args.no_compaction:
         line["compaction_leg"] = compaction_leg(events, counts, tc, first_id, cfg, stream, tallies,
                                                 hbm_peak)
