@@ -163,3 +163,21 @@ def test_graph_and_host_loop_agree(engine):
         out.append(eng.tallies())
         eng.close()
     assert np.array_equal(out[0], out[1])
+
+
+def test_run_batch_with_event_table(engine):
+    """A batch converted once (EventTable) gives the same tallies as the list."""
+    from gpu_optical_photons_b200.wavefront import EventTable
+    events, counts = batched_events(n_events=48, median=2e3)
+    tc = P.TallyConfig(100, 50.0, 10)
+    eng = WavefrontEngine(tc, len(events), int(counts.sum()))
+    try:
+        a, _, _ = eng.run_batch(events, counts)
+        tab = EventTable(events)
+        b, _, _ = eng.run_batch(tab, counts)
+        eng.set_events(tab, counts)
+        eng.run_tally()
+        c = eng.tallies()
+    finally:
+        eng.close()
+    assert np.array_equal(a, b) and np.array_equal(a, c)
