@@ -220,7 +220,8 @@ def adjoint_cost(math: str, n: int = 10_000_000, reps: int = 5) -> dict:
     setup (the Lambertian cube with Rayleigh scattering and a volume source at
     theta = (La 1000, Ls 700, R 0.95, tau 4), 1e7 photons, 500 arrival-time bins):
     median CUDA-event times of the forward tally and of the replay that
-    accumulates dLoss/dtheta, and of the common-random-number central finite
+    accumulates dLoss/dtheta (both the bare C-ABI run, no host read-back inside
+    the events), and of the common-random-number central finite
     differences the adjoint replaces (two forward runs per parameter, at
     theta_j (1 +- 1e-3), parameter upload included)."""
     import torch
@@ -235,6 +236,15 @@ def adjoint_cost(math: str, n: int = 10_000_000, reps: int = 5) -> dict:
         w = torch.ones(tcal.time_bins + 1, dtype=torch.float64)
         m.forward(theta)
         m.replay(theta, w, 0.5)
+        from gpu_optical_photons_b200 import _lib
+        wd = w.cuda()
+        gd = torch.zeros(4, dtype=torch.float64, device="cuda")
+        st = torch.cuda.current_stream().cuda_stream
+
+        def replay_run():
+            _lib.call("optx_engine_run_adjoint", m.engine._h, ctypes.c_void_p(wd.data_ptr()), 0.5,
+                      ctypes.c_void_p(gd.data_ptr()), ctypes.c_void_p(st))
+
         fwd, adj, fd = [], [], []
         for _ in range(reps):
             m._upload(theta)  # back at theta after the FD runs (outside the timed regions)
@@ -242,7 +252,7 @@ def adjoint_cost(math: str, n: int = 10_000_000, reps: int = 5) -> dict:
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(); m.engine.run_tally(); b.record(); torch.cuda.synchronize()
             fwd.append(a.elapsed_time(b))
-            a.record(); m.replay(theta, w, 0.5); b.record(); torch.cuda.synchronize()
+            a.record(); replay_run(); b.record(); torch.cuda.synchronize()
             adj.append(a.elapsed_time(b))
             a.record()
             for j in range(4):

@@ -434,13 +434,13 @@ struct optx_engine {
 
 namespace {
 
-size_t wave_smem(const optx_engine* e, int mode, int variant, bool moments = false) {
+size_t wave_smem(const optx_engine* e, int mode, int variant) {
   const bool batch = variant != kSingle;
   const size_t pantry = static_cast<size_t>(e->cfg.block_size / 32) * kPantryBytesPerWarp;
   if (mode == kModeTally && !batch) return pantry + static_cast<size_t>(e->tdev.len - 7u) * 4u;
-  if (mode == kModeAdjoint)  // bin weights, then (score-moment runs) the block's moment table
+  if (mode == kModeAdjoint || mode == kModeMoments)  // bin weights, then the block's moment table
     return pantry + static_cast<size_t>(e->tdev.time_bins + 1u) * 8u +
-           (moments ? moment_smem_bytes(e->tdev.time_bins) : 0u);
+           (mode == kModeMoments ? moment_smem_bytes(e->tdev.time_bins) : 0u);
   if (mode == kModeTally && batch)  // per-warp event slots
     return pantry + static_cast<size_t>(e->cfg.block_size / 32) *
                         (kSlotCounterBytesPerWarp + slot_bin_bytes_per_warp(e->tdev.len - 7u));
@@ -455,8 +455,8 @@ int engine_minb(const optx_engine* e) {
   return std::max(2, std::min(4, b));
 }
 
-int engine_grid(optx_engine* e, int mode, int batch, int& grid, bool moments = false) {
-  const size_t smem = wave_smem(e, mode, batch, moments);
+int engine_grid(optx_engine* e, int mode, int batch, int& grid) {
+  const size_t smem = wave_smem(e, mode, batch);
   const int math = e->cfg.math;
   const int minb = engine_minb(e);
   int dev = 0, max_smem = 0;
@@ -514,8 +514,8 @@ int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphC
     a.inv_tau2 = theta_inv[6];
   }
   a.score_mask = score_mask;
-  a.grad = (mode == kModeAdjoint) ? e->d_grad : nullptr;
-  a.moments = (mode == kModeAdjoint) ? moments : nullptr;
+  a.grad = (mode == kModeAdjoint || mode == kModeMoments) ? e->d_grad : nullptr;
+  a.moments = (mode == kModeMoments) ? moments : nullptr;
   a.moments_smem = (a.moments != nullptr && moment_smem_bytes(e->tdev.time_bins) != 0u) ? 1u : 0u;
   a.graph_handle = h;
   // Watchdog: no warp can iterate more than (photons + queue) x (max_steps + 2) times.
@@ -543,9 +543,8 @@ int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphC
   return OPTX_OK;
 }
 
-int engine_graph(optx_engine* e, int mode, int batch, int grid, optx_engine::Graph** out,
-                 bool moments = false) {
-  const size_t smem = wave_smem(e, mode, batch, moments);
+int engine_graph(optx_engine* e, int mode, int batch, int grid, optx_engine::Graph** out) {
+  const size_t smem = wave_smem(e, mode, batch);
   const DevParams P0 = batch == kBatch ? DevParams{} : e->P0;
   for (auto& g : e->graphs) {
     if (g.mode == mode && g.batch == batch && g.grid == grid && g.block == e->cfg.block_size &&
@@ -628,12 +627,12 @@ int engine_run(optx_engine* e, int mode, const DevRecords* rec, const double* w_
   // Gensteps always run batched: each lane reads its genstep's record at emission.
   const int batch = (e->n_events > 1 || e->gensteps) ? (e->uniform ? kBatchUniform : kBatch) : kSingle;
   int grid = 0;
-  OPTX_TRY(engine_grid(e, mode, batch, grid, moments != nullptr));
-  const size_t smem = wave_smem(e, mode, batch, moments != nullptr);
+  OPTX_TRY(engine_grid(e, mode, batch, grid));
+  const size_t smem = wave_smem(e, mode, batch);
   const int math = e->cfg.math;
   if (e->cfg.use_graph >= 0) {
     optx_engine::Graph* g = nullptr;
-    OPTX_TRY(engine_graph(e, mode, batch, grid, &g, moments != nullptr));
+    OPTX_TRY(engine_graph(e, mode, batch, grid, &g));
     OPTX_TRY(engine_upload_args(e, mode, batch, grid, g->handle, rec, w_bin, w_det, theta_inv,
                                 score_mask, st, moments));
     OPTX_TRY(engine_device_total(e, st));
@@ -1645,10 +1644,12 @@ int optx_engine_run_score_moments(optx_engine* e, double* dev_moments, void* str
     return fail(OPTX_ERR_INVALID_ARGUMENT, "engine and dev_moments must not be NULL");
   if ((reinterpret_cast<uintptr_t>(dev_moments) & 7u) != 0u)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "dev_moments must be 8-byte aligned");
+  if (e->n_events != 1 || e->gensteps)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "score moments run on one configuration (one event, no gensteps)");
   double inv[7];
   uint32_t mask = 0;
   OPTX_TRY(adjoint_setup(e, inv, mask));
-  return engine_run(e, kModeAdjoint, nullptr, nullptr, 0.0, inv, mask,
+  return engine_run(e, kModeMoments, nullptr, nullptr, 0.0, inv, mask,
                     static_cast<cudaStream_t>(stream), dev_moments);
 }
 

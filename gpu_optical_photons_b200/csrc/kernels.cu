@@ -250,6 +250,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
   //  or, batched tally, per-warp event slots: nwarps x 2 x 8 u64 counters, then
   //  nwarps x 2 x n_bins u32 bins when n_bins <= kSlotBins]
   constexpr bool kSlots = BATCH && MODE == kModeTally;
+  constexpr bool kAdj = MODE == kModeAdjoint || MODE == kModeMoments;  // replay modes
   float4* pantry = reinterpret_cast<float4*>(smem_raw + warp * kPantryBytesPerWarp);
   unsigned char* extra = smem_raw + nwarps * kPantryBytesPerWarp;
   uint32_t* s_hist = reinterpret_cast<uint32_t*>(extra);
@@ -317,10 +318,10 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
       for (uint32_t b = lane; b < 2u * n_bins; b += 32u) s_sb[b] = 0u;
     }
   }
-  if (MODE == kModeAdjoint) {
+  if (kAdj) {
     const double* wb = A->w_bin;
     for (uint32_t b = threadIdx.x; b <= tc.time_bins; b += blockDim.x) s_w[b] = wb ? wb[b] : 0.0;
-    if (A->moments_smem) {
+    if (MODE == kModeMoments && A->moments_smem) {
       for (uint32_t i = threadIdx.x; i < 5u * (tc.time_bins + 1u); i += blockDim.x) s_mom[i] = 0.0;
     }
   }
@@ -425,7 +426,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
       if (fate == kDetected) {
         const uint32_t tb = time_bin(s.t, tc.tscale, tc.time_bins);
         const double w = s_w[tb] + A->w_det;
-        double* M = A->moments;
+        double* M = MODE == kModeMoments ? A->moments : nullptr;
         if (w != 0.0 || M != nullptr) {
           const double path = s.path;
           const uint32_t m = A->score_mask;
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
           g2 += w * s2;
           g3 += w * s3;
           if (M != nullptr) {  // per-bin (count, score sums): histogram and Jacobian in one pass
-            double* mb = (A->moments_smem ? s_mom : M) + 5u * tb;
+            double* mb = (MODE == kModeMoments && A->moments_smem ? s_mom : M) + 5u * tb;
             atomicAdd(mb, 1.0);
             if (s0 != 0.0) atomicAdd(mb + 1, s0);
             if (s1 != 0.0) atomicAdd(mb + 2, s1);
@@ -526,7 +527,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
             ns.nb = __float_as_uint(c.x);
             ns.ns = __float_as_uint(c.y);
             npidx = __float_as_uint(c.w);
-            if (MODE == kModeAdjoint) {
+            if (kAdj) {
               na_aux.n_refl = __float_as_uint(d.x);
               na_aux.t_emit = d.y;
             }
@@ -540,7 +541,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
             const DevParams& R = BATCH ? A->params[nev] : P0;  // the photon's record
             nr.init(first_id + g, R.key_lo, R.key_hi, 0u);
             const float4* sg = A->seg == nullptr ? nullptr : A->seg + 2u * nev;
-            start_photon<MODE == kModeAdjoint>(R, ns, nr, first_id + g, na_aux, sg);
+            start_photon<kAdj>(R, ns, nr, first_id + g, na_aux, sg);
             if (BATCH) nev = event_of(nev);  // from here on the photon needs only its event
           }
           float4* e = pantry + (pc + lane) * 7u;
@@ -549,7 +550,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
           e[2] = make_uint4_as_float4(ns.nb, ns.ns, npidx, nev);
           e[3] = make_uint4_as_float4(nr.w[0], nr.w[1], nr.w[2], nr.w[3]);
           e[4] = make_uint4_as_float4(nr.w[4], nr.w[5], nr.w[6], nr.w[7]);
-          if (MODE == kModeAdjoint) {
+          if (kAdj) {
             e[5] = make_float4(__uint_as_float(nr.o), __uint_as_float(nr.blk),
                                __uint_as_float(na_aux.n_refl), na_aux.t_emit);
           } else {
@@ -589,7 +590,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
           r.w[2] = __float_as_uint(d.z); r.w[3] = __float_as_uint(d.w);
           r.w[4] = __float_as_uint(f.x); r.w[5] = __float_as_uint(f.y);
           r.w[6] = __float_as_uint(f.z); r.w[7] = __float_as_uint(f.w);
-          if (MODE == kModeAdjoint) {
+          if (kAdj) {
             const float4 h = e[5];
             r.o = __float_as_uint(h.x);
             r.blk = __float_as_uint(h.y);
@@ -634,7 +635,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     if (alive) {
       const DevParams& P = params_of<BATCH, UNI>(P0, A, ev);
       const bool still =
-          step_photon<MODE == kModeAdjoint>(P, s, r, first_id + pidx, fate, aux, smask);
+          step_photon<kAdj>(P, s, r, first_id + pidx, fate, aux, smask);
       ++wsteps;
       ended = !still || s.nb + s.ns >= P.max_steps;  // at max_steps fate stays kMaxSteps
     }
@@ -680,7 +681,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
       }
     }
   }
-  if (MODE == kModeAdjoint) {
+  if (kAdj) {
     g0 = warp_sum_f64(g0);
     g1 = warp_sum_f64(g1);
     g2 = warp_sum_f64(g2);
@@ -697,7 +698,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
       for (uint32_t w = 0; w < nwarps; ++w) acc += s_red[threadIdx.x][w];
       if (acc != 0.0) atomicAdd(&A->grad[threadIdx.x], acc);
     }
-    if (A->moments_smem) {  // every lane's moments are in s_mom (barrier above)
+    if (MODE == kModeMoments && A->moments_smem) {  // every lane's moments are in s_mom (barrier above)
       double* M = A->moments;
       for (uint32_t i = threadIdx.x; i < 5u * (tc.time_bins + 1u); i += blockDim.x) {
         if (s_mom[i] != 0.0) atomicAdd(M + i, s_mom[i]);
@@ -803,6 +804,8 @@ const void* wave_kernel_fn(int mode, int batch, int minb) {
   switch (mode) {
     case kModeTally: return kfn_variant<kModeTally>(batch, minb);
     case kModeRecords: return kfn_variant<kModeRecords>(batch, minb);
+    case kModeMoments:  // single configuration only (the host checks)
+      return batch == kSingle ? kfn<kModeMoments, false, false>(minb) : nullptr;
     default: return kfn_variant<kModeAdjoint>(batch, minb);
   }
 }

@@ -77,7 +77,9 @@ struct WaveCtrl {
                                    // photons than the engine holds (kept until the next upload)
 };
 
-enum WaveMode : int { kModeTally = 0, kModeRecords = 1, kModeAdjoint = 2 };
+// kModeMoments: the adjoint replay that also fills the per-bin score moments
+// (single configuration only; a kernel of its own keeps the gradient replay lean).
+enum WaveMode : int { kModeTally = 0, kModeRecords = 1, kModeAdjoint = 2, kModeMoments = 3 };
 // Wave kernel variants: one configuration (physics in the kernel argument); a
 // batch of records with per-event physics; a batch whose events share their
 // step physics (kernel argument), with per-record emission and per-event tallies.
