@@ -241,7 +241,8 @@ int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* s
  * optx_engine_stats / optx_engine_get_tallies on the engine. */
 int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_det,
                             double* dev_grad, void* stream);
-/* Per-bin score moments (extension, same replay as optx_engine_run_adjoint):
+/* Per-bin score moments (extension, same replay as optx_engine_run_adjoint, on
+ * an engine holding one configuration: one event, no gensteps):
  * for each arrival-time bin b (time_bins + 1 entries, the last = overflow)
  *   moments[5 b + 0] = detected photons in b  (the run's histogram h_b)
  *   moments[5 b + 1 + j] = sum over them of S_j
