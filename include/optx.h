@@ -214,7 +214,9 @@ int optx_engine_set_gensteps(optx_engine* e, const optx_params* events, const op
  * holds, is reported as OPTX_ERR_INVALID_ARGUMENT by the next
  * optx_engine_get_tallies / optx_engine_stats (the run then tallies without
  * the invalid gensteps, or nothing when over capacity). Results equal those of
- * optx_engine_set_gensteps with the same gensteps. */
+ * optx_engine_set_gensteps with the same gensteps. The photon total is known on
+ * the device only: records arrays for optx_engine_run_records must hold the
+ * engine's max_photons entries (those past the total are left untouched). */
 int optx_engine_set_gensteps_device(optx_engine* e, const optx_params* events,
                                     const optx_faces* faces, uint32_t n_events,
                                     const optx_genstep* dev_gensteps, uint32_t n_gensteps,
