@@ -333,15 +333,19 @@ def run_reference(args):
     rg = reference_gpu_leg(events, counts, tc)
     if rg is not None:
         line["reference_gpu"] = rg
+    rs = reference_gpu_single_configs()
+    if rs is not None:
+        line["reference_gpu_single_configs"] = rs
     print(json.dumps(line), flush=True)
 
 
 def single_config_legs(math: str, n: int = 100_000_000, reps: int = 3) -> dict:
     """One configuration at its specified size (the wrapped-Lambertian cube with
     Rayleigh scattering and the all-specular long bar, 1e8 photons each, tally
-    mode): the wavefront engine (host-call settings: 7 blocks of 128 threads),
-    this library's history kernel and, when built, the reference's tally kernel
-    on the same GPU. Median CUDA-event kernel times."""
+    mode): the wavefront engine (host-call settings: 7 blocks of 128 threads)
+    and this library's history kernel. Median CUDA-event kernel times. (The
+    reference's own kernels on the same workloads are timed by the reference
+    arm, `--impl reference`.)"""
     import torch
     from gpu_optical_photons_b200 import backend as B
     from gpu_optical_photons_b200.params import config2, config3
@@ -357,13 +361,6 @@ def single_config_legs(math: str, n: int = 100_000_000, reps: int = 3) -> dict:
             ts.append(a.elapsed_time(b))
         return float(np.median(ts))
 
-    O = None
-    try:
-        from oracle import oracle as O
-        if not O.refgpu_available():
-            O = None
-    except Exception:
-        O = None
     out = {}
     for name, (p, c) in (("wrapped_lambertian_rayleigh", config2()), ("long_bar_specular", config3(False))):
         eng = WavefrontEngine(c, 1, n, WaveConfig(blocks_per_sm=7, math=math))
@@ -376,12 +373,8 @@ def single_config_legs(math: str, n: int = 100_000_000, reps: int = 3) -> dict:
         steps = int(t[-2] + t[-1] + t[1])
         dev = torch.zeros(c.length, dtype=torch.int64, device="cuda")
         hist = ev_ms(lambda: B.tally_device(p, c, n, out=dev, math=math))
-        row = {"photons": n, "photon_steps": steps, "wavefront_ms": wave, "history_ms": hist,
-               "wavefront_photon_steps_per_s": steps / (wave * 1e-3)}
-        if O is not None and math == "fast":
-            row["reference_kernel_ms"] = float(np.median([O.refgpu_tally(p, c, n)[1]["kernel_ms"]
-                                                          for _ in range(reps)]))
-        out[name] = row
+        out[name] = {"photons": n, "photon_steps": steps, "wavefront_ms": wave, "history_ms": hist,
+                     "wavefront_photon_steps_per_s": steps / (wave * 1e-3)}
     return out
 
 
@@ -416,6 +409,31 @@ def reference_gpu_leg(events, counts, tc):
             "kernel_only_value": steps / (kms * 1e-3), "kernel_ms_per_step": kms, "calls": int((counts > 0).sum()),
             "what": "reference src/gpu/gpu_backend.cu built for sm_100a from its sources; run_gpu_tally per event "
                     "(host buffers, allocation per call), same 4096-event batch and tally binning"}
+
+
+def reference_gpu_single_configs(n: int = 100_000_000, reps: int = 3):
+    """The reference's tally kernel (rebuilt for sm_100a) on the single
+    configurations the optx arm's `single_configs` key times (1e8 photons each):
+    median kernel time reported by its run_gpu_tally. None without the library
+    or a GPU."""
+    from oracle import oracle as O
+    try:
+        import torch
+        if not (O.refgpu_available() and torch.cuda.is_available()):
+            return None
+    except Exception:
+        return None
+    from gpu_optical_photons_b200.params import config2, config3
+    out = {}
+    for name, (p, c) in (("wrapped_lambertian_rayleigh", config2()), ("long_bar_specular", config3(False))):
+        O.refgpu_tally(p, c, n)  # warm-up
+        runs = [O.refgpu_tally(p, c, n) for _ in range(reps)]
+        t = runs[0][0]
+        steps = steps_of_tallies(t[None, :])
+        kms = float(np.median([tm["kernel_ms"] for _, tm in runs]))
+        out[name] = {"photons": n, "photon_steps": steps, "kernel_ms": kms,
+                     "kernel_photon_steps_per_s": steps / (kms * 1e-3)}
+    return out
 
 
 def run_optx(args):
