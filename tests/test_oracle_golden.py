@@ -43,6 +43,20 @@ def test_fresnel_normal_incidence(oracle):
     assert oracle.lib().oracle_fresnel(1.63, 1.0, 0.2) == 1.0           # TIR
 
 
+@pytest.mark.parametrize("mode", [0, 1])  # platform (libm) and portable math
+def test_rayleigh_cos_inverts_its_cdf(oracle, mode):
+    # tests/test_sampling.cpp:90-101: F(mu) = (mu^3 + 3 mu + 4) / 8 inverts the
+    # Cardano sampler to 2e-6 on u = i / 1000, mu stays in [-1, 1].
+    f = oracle.lib().oracle_rayleigh_cos
+    for i in range(1, 1001):
+        u = i / 1000.0
+        mu = float(f(u, mode))
+        assert -1.0 <= mu <= 1.0
+        assert abs((mu ** 3 + 3.0 * mu + 4.0) / 8.0 - float(np.float32(u))) <= 2e-6, (u, mu)
+    assert abs(float(f(0.5, mode))) <= 1e-7
+    assert abs(float(f(1.0, mode)) - 1.0) <= 1e-6
+
+
 CASES = ["default", "default_scat300_volume", "config1", "config2", "config3_all_specular",
          "black_box", "absorption", "mirror_box", "capped", "big_seed_id"]
 
