@@ -43,6 +43,56 @@ def test_fresnel_normal_incidence(oracle):
     assert oracle.lib().oracle_fresnel(1.63, 1.0, 0.2) == 1.0           # TIR
 
 
+def test_fresnel_brewster_and_angle_form(oracle):
+    # tests/test_fresnel.cpp:76-96: at Brewster's angle Rp = 0, so R = Rs / 2;
+    # over 0.5..89.5 degrees R agrees with the angle-form expressions to 2e-5.
+    import math
+    f = oracle.lib().oracle_fresnel
+    tb = math.atan(1.63 / 1.0)
+    tt = math.asin(1.0 / 1.63 * math.sin(tb))
+    rs = math.sin(tb - tt) / math.sin(tb + tt)
+    assert abs(f(1.0, 1.63, math.cos(tb)) - 0.5 * rs * rs) <= 1e-6
+
+    def angle_form(n1, n2, th):
+        s = n1 / n2 * math.sin(th)
+        if s >= 1.0:
+            return 1.0
+        tt = math.asin(s)
+        if th == 0.0:
+            return ((n1 - n2) / (n1 + n2)) ** 2
+        a = math.sin(th - tt) / math.sin(th + tt)
+        b = math.tan(th - tt) / math.tan(th + tt)
+        return 0.5 * (a * a + b * b)
+
+    for n1, n2 in ((1.63, 1.0), (1.0, 1.63), (1.63, 1.5), (1.5, 1.63)):
+        for k in range(1, 180):
+            th = math.radians(0.5 * k)
+            got = f(n1, n2, float(np.float32(math.cos(th))))
+            assert abs(got - angle_form(n1, n2, th)) <= 2e-5, (n1, n2, 0.5 * k, got)
+
+
+def test_streams_differ_and_are_uniform(oracle):
+    # tests/test_rng.cpp:73-118: different photons and seeds give different
+    # streams; the first four deviates of 250k consecutive photon streams are
+    # uniform (chi2 p > 1e-4, mean within 5 sigma) and neighbouring streams'
+    # first deviates are uncorrelated.
+    from scipy import stats
+    a, b, c = oracle.stream(1, 0, 1000), oracle.stream(1, 1, 1000), oracle.stream(2, 0, 1000)
+    assert (a == b).sum() <= 1 and (a == c).sum() <= 1
+    n_ph = 250_000
+    w = np.stack([oracle.stream(777, i, 4) for i in range(n_ph)])
+    u = (((w >> 8) + 1).astype(np.float64) * 2.0 ** -24)
+    assert u.min() > 0.0 and u.max() <= 1.0
+    n = u.size
+    assert abs(u.mean() - 0.5) < 5.0 * np.sqrt(1.0 / 12.0 / n)
+    first = u[:, 0] - 0.5
+    corr = float((first[1:] * first[:-1]).sum() / n_ph) * 12.0
+    assert abs(corr) < 5.0 / np.sqrt(n_ph)
+    hist = np.bincount(np.minimum((u.ravel() * 100).astype(int), 99), minlength=100)
+    chi2 = float((((hist - n / 100) ** 2) / (n / 100)).sum())
+    assert stats.chi2.sf(chi2, 99) > 1e-4
+
+
 @pytest.mark.parametrize("mode", [0, 1])  # platform (libm) and portable math
 def test_rayleigh_cos_inverts_its_cdf(oracle, mode):
     # tests/test_sampling.cpp:90-101: F(mu) = (mu^3 + 3 mu + 4) / 8 inverts the
