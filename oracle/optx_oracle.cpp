@@ -600,6 +600,24 @@ float oracle_rayleigh_cos(float u, int mode) {
                    : sample_rayleigh_cos<float, PlatformMath>(u);
 }
 
+// The direction samplers of the transport (sampling.hpp:22-56), for tests:
+// kind 0 isotropic (cos theta = 2 u1 - 1, azimuth u2 turns); kind 1 Lambertian
+// about the unit axis a (cos theta = sqrt(u1)); kind 2 Rayleigh scattering of
+// the unit direction a (cos theta from the Cardano sampler). Platform math.
+void oracle_sample_direction(int kind, float u1, float u2, const float* a, float* out) {
+  V3<float> d{};
+  if (kind == 0) {
+    d = sample_isotropic<float, PlatformMath>(u1, u2);
+  } else {
+    const V3<float> axis{a[0], a[1], a[2]};
+    const float ct = kind == 1 ? sqrt_(u1) : sample_rayleigh_cos<float, PlatformMath>(u1);
+    d = rotate_about<float, PlatformMath>(axis, ct, u2);
+  }
+  out[0] = d.x;
+  out[1] = d.y;
+  out[2] = d.z;
+}
+
 // Records for photons first_id .. first_id + n - 1. Any output pointer may be null.
 int oracle_records(const Params* p, const Faces* faces, uint64_t n, uint64_t first_id, int mode,
                    int threads, uint8_t* fate, uint32_t* nb, uint32_t* ns, float* t, float* x,

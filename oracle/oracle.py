@@ -53,6 +53,7 @@ def lib():
         L.oracle_adjoint.argtypes = [_P, _P, _u64, _u64, ctypes.c_int, ctypes.c_int, _P,
                                      ctypes.c_double, _P, _P, _P]
         L.oracle_score_moments.argtypes = [_P, _P, _u64, _u64, ctypes.c_int, ctypes.c_int, _P]
+        L.oracle_sample_direction.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float, _P, _P]
         L.oracle_opcount.argtypes = [_P, _P, _u64, _u64, _P]
         L.oracle_stream.argtypes = [_u64, _u64, ctypes.c_uint32, ctypes.c_uint32, _P]
         L.oracle_philox.argtypes = [_P, _P, _P]
