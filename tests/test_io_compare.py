@@ -176,3 +176,27 @@ def test_cli_records_out_against_reference_cpu(oracle, tmp_path):
     assert res["history"]["fate_differs"] <= 0.001 * n
     assert abs(res["distribution"]["eff_z"]) < 4.0
     assert IO.read_meta(str(d_gpu))["backend"] == "gpu"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("argv", [
+    ["--config", "config2", "--engine", "history", "--n", "2e5"],
+    ["--config", "config3", "--engine", "wave", "--n", "2e5", "--bps", "7"],
+    ["--config", "config1", "--engine", "wave", "--n", "2e5", "--cadence", "8", "--host-loop"],
+    ["--engine", "gensteps", "--n", "16"],
+])
+def test_cli_engines_print_a_consistent_line(engine, capsys, tmp_path, argv):
+    """Every engine of the command-line runner prints one JSON line whose fates
+    add up to the photons it ran (and, with --out, writes a tally the reader
+    gives back)."""
+    import json
+    from gpu_optical_photons_b200 import cli
+    out_dir = tmp_path / "t"
+    gs = "gensteps" in argv
+    cli.main(argv + ["--repeat", "2"] + ([] if gs else ["--out", str(out_dir)]))
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    n = line.get("photons", line["n"])
+    assert sum(line["fates"]) == n and line["steps"] > 0 and line["ms"] > 0
+    if not gs:
+        t = IO.read_tally(str(out_dir))
+        assert int(np.asarray(t.fate_counts).sum()) == n
