@@ -342,14 +342,16 @@ def run_reference(args):
 def single_config_legs(math: str, n: int = 100_000_000, reps: int = 3) -> dict:
     """One configuration at its specified size (the wrapped-Lambertian cube with
     Rayleigh scattering and the all-specular long bar, 1e8 photons each, tally
-    mode): the wavefront engine (host-call settings: 7 blocks of 128 threads)
-    and this library's history kernel. Median CUDA-event kernel times. (The
+    mode): the wavefront engine (host-call settings: 7 blocks of 128 threads),
+    the per-interaction sorted kernels (photons queued in HBM by pending
+    interaction, one launch per iteration) and this library's history kernel.
+    Median CUDA-event kernel times. (The
     reference's own kernels on the same workloads are timed by the reference
     arm, `--impl reference`.)"""
     import torch
     from gpu_optical_photons_b200 import backend as B
     from gpu_optical_photons_b200.params import config2, config3
-    from gpu_optical_photons_b200.wavefront import WaveConfig, WavefrontEngine
+    from gpu_optical_photons_b200.wavefront import SortedEngine, WaveConfig, WavefrontEngine
 
     def ev_ms(fn):
         fn()
@@ -373,7 +375,14 @@ def single_config_legs(math: str, n: int = 100_000_000, reps: int = 3) -> dict:
         steps = int(t[-2] + t[-1] + t[1])
         dev = torch.zeros(c.length, dtype=torch.int64, device="cuda")
         hist = ev_ms(lambda: B.tally_device(p, c, n, out=dev, math=math))
+        srt = SortedEngine(math=math)
+        try:
+            sorted_ms = ev_ms(lambda: srt.run(p, n, tally=c, tally_out=dev))
+            sst = srt.stats()
+        finally:
+            srt.close()
         out[name] = {"photons": n, "photon_steps": steps, "wavefront_ms": wave, "history_ms": hist,
+                     "sorted_ms": sorted_ms, "sorted_iterations": sst["iterations"],
                      "wavefront_photon_steps_per_s": steps / (wave * 1e-3)}
     return out
 

@@ -14,7 +14,8 @@ from ._lib import OptxError, InvalidArgument
 from .backend import (Records, Tally, gpu_available, gpu_device_name, run_gpu_records,
                       run_gpu_tally, run_gpu_records_event, records_device, tally_device,
                       device_records, records_to_numpy)
-from .wavefront import EventTable, WavefrontEngine, WaveConfig, wavefront_tally, batched_events
+from .wavefront import (EventTable, SortedEngine, WavefrontEngine, WaveConfig, wavefront_tally,
+                        batched_events)
 
 
 def __getattr__(name):

@@ -59,6 +59,21 @@ class CEventStats(ctypes.Structure):
         return d
 
 
+class CSortedConfig(ctypes.Structure):
+    _fields_ = [("capacity", ctypes.c_uint32), ("drain_below", ctypes.c_uint32), ("math", ctypes.c_int32),
+                ("blocks_per_sm", ctypes.c_int32), ("host_loop", ctypes.c_uint32)]
+
+
+class CSortedCounters(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_uint64), ("queued", ctypes.c_uint64 * 3),
+                ("drained", ctypes.c_uint64), ("kernel_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {"iterations": self.iterations,
+                "queued": dict(zip(("scatter", "polished", "painted"), list(self.queued))),
+                "drained": self.drained, "kernel_ms": self.kernel_ms}
+
+
 class CWaveConfig(ctypes.Structure):
     _fields_ = [("block_size", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
                 ("threshold", ctypes.c_uint32), ("cadence", ctypes.c_uint32),
@@ -100,6 +115,10 @@ _SIGS = {
     "optx_engine_run_adjoint": [_P, _P, ctypes.c_double, _P, _P],
     "optx_engine_run_score_moments": [_P, _P, _P],
     "optx_wavefront_tally_noalloc": [_P, _P, _P, _u64, _u64, _P, _int, _P],
+    "optx_sorted_create": [_P, _P],
+    "optx_sorted_destroy": [_P],
+    "optx_sorted_run": [_P, _P, _P, _P, _u64, _u64, _P, _P, _P],
+    "optx_sorted_stats": [_P, _P, _P],
     "optx_engine_tally_ptr": [_P, _P, _P],
     "optx_engine_get_tallies": [_P, _P, _P],
     "optx_engine_stats": [_P, _P, _P],

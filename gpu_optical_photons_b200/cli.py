@@ -1,8 +1,10 @@
 """Command-line runner (the role of the reference's apps/optphot_main.cpp and
 apps/optphot_event_bench.cpp): runs one configuration through the history or
-the wavefront kernel and prints a JSON line with timings and tallies summary.
+the wavefront kernel (or the per-interaction sorted kernels, or gensteps through
+the wavefront engine) and prints a JSON line with timings and tallies summary.
 
     python -m gpu_optical_photons_b200.cli --config config2 --engine wave --n 1e7
+    python -m gpu_optical_photons_b200.cli --config config2 --engine sorted --n 1e7
     python -m gpu_optical_photons_b200.cli --config config1 --engine history --mode records --n 1e6
 
 Options mirror the reference's physics keys (--n_det, --abs_length, ...).
@@ -26,7 +28,7 @@ CONFIGS = {"default": lambda: (P.SimParams(), P.TallyConfig()),
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--config", default="config1", choices=sorted(CONFIGS))
-    ap.add_argument("--engine", default="history", choices=["history", "wave", "gensteps"],
+    ap.add_argument("--engine", default="history", choices=["history", "wave", "sorted", "gensteps"],
                     help="gensteps: --n straight muon tracks through the cube (1 mm gensteps, "
                          "200 photons/mm) expanded into photons by the wavefront engine")
     ap.add_argument("--mode", default="tally", choices=["tally", "records"])
@@ -36,9 +38,12 @@ def main(argv=None):
     ap.add_argument("--threshold", type=int, default=28)
     ap.add_argument("--cadence", type=int, default=0)
     ap.add_argument("--bps", type=int, default=0, help="wave engine register budget: 2/3/4 (blocks of "
-                    "256) or 7 (blocks of 128); 0 = default")
+                    "256) or 7 (blocks of 128); sorted engine: 3 or 4; 0 = default")
     ap.add_argument("--chunk", type=int, default=0)
-    ap.add_argument("--host-loop", action="store_true", help="launch waves from the host (no graph)")
+    ap.add_argument("--host-loop", action="store_true",
+                    help="launch waves (sorted: iterations) from the host (no graph)")
+    ap.add_argument("--capacity", type=int, default=0,
+                    help="sorted engine: photons in flight (default 2^21)")
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--out", help="write records / tally .npy files and meta.json here "
                     "(the reference's optphot --out layout)")
@@ -95,6 +100,30 @@ def main(argv=None):
                 g.records_device(p, n, out=rec, block_size=a.block, math=a.math)
                 torch.cuda.synchronize()
                 times.append((time.perf_counter() - t0) * 1e3)
+            r = g.records_to_numpy(rec)
+            flat = None
+            out["steps"] = int(r.steps().sum())
+            if a.out:
+                from . import io
+                meta = io.params_to_json(p, io.RunOptions("gpu", "records", n, 1, a.block, c))
+                io.write_records(a.out, r, meta)
+    elif a.engine == "sorted":
+        from .wavefront import SortedEngine
+        eng = SortedEngine(a.capacity, 0, a.math, host_loop=a.host_loop, blocks_per_sm=a.bps)
+        dev = torch.zeros(c.length, dtype=torch.int64, device="cuda") if a.mode == "tally" else None
+        rec = g.device_records(n) if a.mode == "records" else None
+        for _ in range(a.repeat):
+            if dev is not None:
+                dev.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.run(p, n, tally=c if dev is not None else None, tally_out=dev, records_out=rec)
+            out["sorted"] = eng.stats()  # synchronises
+            times.append((time.perf_counter() - t0) * 1e3)
+        eng.close()
+        if dev is not None:
+            flat = dev.cpu().numpy().astype(np.uint64)
+        else:
             r = g.records_to_numpy(rec)
             flat = None
             out["steps"] = int(r.steps().sum())

@@ -1781,6 +1781,243 @@ int optx_run_records_event(const optx_params* p, const optx_faces* faces, uint64
 }  // extern "C"
 
 // =============================================================================
+// Per-interaction sorted run: state queues per pending interaction, one launch
+// per iteration inside a CUDA-graph while loop (kernels.cu, sorted_kernel).
+struct optx_sorted {
+  std::mutex mu;
+  int math = OPTX_MATH_FAST;
+  int minb = 3;  // resident blocks per SM (register budget)
+  uint32_t cap = 0, drain_below = 0;
+  bool host_loop = false;
+  int grid = 0;
+  unsigned char* d_mem = nullptr;  // queues, ids and the control block in one allocation
+  SortCtrl* d_ctrl = nullptr;
+  float4* q[2][kSortQueues] = {};
+  uint32_t* qid[2][kSortQueues] = {};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool ran = false;
+  // The run's configuration and arguments are kernel parameters, so a graph
+  // belongs to one (P, args) pair; repeated runs of the same work reuse it.
+  struct Graph {
+    DevParams P;
+    SortArgs A;  // graph_handle zeroed in the key
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Graph> graphs;
+};
+
+namespace {
+
+constexpr int kSortBlock = kSortThreads;
+constexpr uint32_t kSortDefaultCap = 1u << 21;
+
+int sorted_free(optx_sorted* s) {
+  for (auto& g : s->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+  }
+  cudaFree(s->d_mem);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  delete s;
+  return OPTX_OK;
+}
+
+// The run's graph: prep (control block), then while (photons left) { iteration }.
+int sorted_graph(optx_sorted* s, const DevParams& P, const SortArgs& key, optx_sorted::Graph** out) {
+  for (auto& g : s->graphs) {
+    if (std::memcmp(&g.P, &P, sizeof(P)) == 0 && std::memcmp(&g.A, &key, sizeof(key)) == 0) {
+      *out = &g;
+      return OPTX_OK;
+    }
+  }
+  optx_sorted::Graph g{};
+  g.P = P;
+  g.A = key;
+  cudaGraphConditionalHandle handle;
+  OPTX_CUDA(cudaGraphCreate(&g.graph, 0));
+  OPTX_CUDA(cudaGraphConditionalHandleCreate(&handle, g.graph, 1u, cudaGraphCondAssignDefault));
+  SortArgs a = key;
+  a.graph_handle = handle;
+  a.use_graph = 1u;
+  SortCtrl* c_ptr = s->d_ctrl;
+  void* prep_args[] = {&a, &c_ptr};
+  cudaKernelNodeParams kp{};
+  kp.func = const_cast<void*>(DISPATCH(s->math, sorted_prep_fn));
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(32);
+  kp.kernelParams = prep_args;
+  cudaGraphNode_t n_prep;
+  OPTX_CUDA(cudaGraphAddKernelNode(&n_prep, g.graph, nullptr, 0, &kp));
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t n_while;
+  OPTX_CUDA(cudaGraphAddNode(&n_while, g.graph, &n_prep, 1, &cp));
+  DevParams p_copy = P;
+  void* it_args[] = {&p_copy, &a, &c_ptr};
+  cudaKernelNodeParams ip{};
+  ip.func = const_cast<void*>(DISPATCH(s->math, sorted_kernel_fn, s->minb));
+  ip.gridDim = dim3(s->grid);
+  ip.blockDim = dim3(kSortBlock);
+  ip.kernelParams = it_args;
+  cudaGraphNode_t n_it;
+  OPTX_CUDA(cudaGraphAddKernelNode(&n_it, cp.conditional.phGraph_out[0], nullptr, 0, &ip));
+  OPTX_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+  constexpr size_t kMaxGraphs = 8;
+  if (s->graphs.size() >= kMaxGraphs) {
+    cudaGraphExecDestroy(s->graphs.front().exec);
+    cudaGraphDestroy(s->graphs.front().graph);
+    s->graphs.erase(s->graphs.begin());
+  }
+  s->graphs.push_back(g);
+  *out = &s->graphs.back();
+  return OPTX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int optx_sorted_create(const optx_sorted_config* cfg, optx_sorted** out) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (out == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "out must not be NULL");
+  *out = nullptr;
+  const optx_sorted_config k = cfg != nullptr ? *cfg : optx_sorted_config{};
+  OPTX_TRY(check_math(k.math));
+  if (k.host_loop != 0u && k.host_loop != 1u)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "host_loop must be 0 or 1");
+  if (k.blocks_per_sm != 0 && k.blocks_per_sm != 3 && k.blocks_per_sm != 4)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "blocks_per_sm must be 0, 3 or 4");
+  const uint64_t cap = k.capacity == 0u ? kSortDefaultCap : ((uint64_t(k.capacity) + 31u) & ~uint64_t(31));
+  if (cap > (1ull << 28)) return fail(OPTX_ERR_INVALID_ARGUMENT, "capacity must be <= 2^28 photons");
+  OPTX_TRY(ensure_device());
+  const int minb = k.blocks_per_sm != 0 ? k.blocks_per_sm : 3;
+  const int bps = DISPATCH(k.math, sorted_blocks_per_sm, minb, kSortBlock);
+  if (bps <= 0) return fail(OPTX_ERR_RUNTIME, "sorted kernel cannot be resident");
+  optx_sorted* s = new optx_sorted();
+  s->math = k.math;
+  s->minb = minb;
+  s->host_loop = k.host_loop != 0u;
+  s->cap = static_cast<uint32_t>(cap);
+  s->grid = bps * num_sms();
+  s->drain_below = k.drain_below != 0u ? k.drain_below : static_cast<uint32_t>(s->grid) * kSortBlock;
+  const size_t q_bytes = cap * kSortVec4 * 16ull, id_bytes = cap * 4ull;
+  const size_t ctrl_off = 2ull * kSortQueues * (q_bytes + id_bytes);
+  const size_t total = ctrl_off + sizeof(SortCtrl);
+  cudaError_t err = test_fault("alloc") ? cudaErrorMemoryAllocation
+                                        : cudaMalloc(reinterpret_cast<void**>(&s->d_mem), total);
+  if (err != cudaSuccess) {
+    cudaGetLastError();
+    sorted_free(s);
+    return fail(OPTX_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(err));
+  }
+  size_t off = 0;
+  for (int p = 0; p < 2; ++p)
+    for (uint32_t q = 0; q < kSortQueues; ++q) {
+      s->q[p][q] = reinterpret_cast<float4*>(s->d_mem + off);
+      off += q_bytes;
+      s->qid[p][q] = reinterpret_cast<uint32_t*>(s->d_mem + off);
+      off += id_bytes;
+    }
+  // 128-byte aligned, as SortCounter wants: ctrl_off = 504 bytes x cap, cap a multiple of 32.
+  s->d_ctrl = reinterpret_cast<SortCtrl*>(s->d_mem + ctrl_off);
+  if (cudaMemset(s->d_ctrl, 0, sizeof(SortCtrl)) != cudaSuccess ||
+      cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
+    cudaGetLastError();
+    sorted_free(s);
+    return fail(OPTX_ERR_CUDA, "sorted run set-up failed");
+  }
+  *out = s;
+  return OPTX_OK;
+}
+
+int optx_sorted_destroy(optx_sorted* s) {
+  if (s == nullptr) return OPTX_OK;
+  return sorted_free(s);
+}
+
+int optx_sorted_run(optx_sorted* s, const optx_params* p, const optx_faces* faces,
+                    const optx_tally_config* c, uint64_t n, uint64_t first_id, uint64_t* dev_tally,
+                    const optx_records* dev_records, void* stream) {
+  if (s == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "sorted run must not be NULL");
+  OPTX_TRY(check_params(p, faces));
+  if (dev_tally == nullptr && dev_records == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "give dev_tally, dev_records or both");
+  TallyDev td{};
+  if (dev_tally != nullptr) OPTX_TRY(make_tally_dev(c, td));
+  if (dev_records != nullptr) OPTX_TRY(check_records(dev_records));
+  if (n >= (1ull << 32)) return fail(OPTX_ERR_INVALID_ARGUMENT, "at most 2^32 - 1 photons per run");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (n == 0) return OPTX_OK;
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const DevParams P = make_dev_params(*p, faces);
+  SortArgs a{};  // value-initialised: padding is zero, so the graph key compares bytes
+  for (int q = 0; q < 2; ++q)
+    for (uint32_t k = 0; k < kSortQueues; ++k) {
+      a.q[q][k] = s->q[q][k];
+      a.qid[q][k] = s->qid[q][k];
+    }
+  a.cap = s->cap;
+  a.drain_below = s->drain_below;
+  a.n = n;
+  a.first_id = first_id;
+  a.tally = reinterpret_cast<unsigned long long*>(dev_tally);
+  a.tc = td;
+  if (dev_records != nullptr) a.rec = to_dev(dev_records);
+  // Each photon needs at most max_steps + 1 iterations in flight, and the
+  // queues admit `cap` photons at a time.
+  const unsigned long long bound =
+      (n / s->cap + 2ull) * (static_cast<unsigned long long>(P.max_steps) + 2ull) + 64ull;
+  a.iter_cap = test_fault("watchdog") ? 1u : static_cast<uint32_t>(std::min(bound, 0xfffffff0ull));
+  OPTX_CUDA(cudaEventRecord(s->ev0, st));
+  s->ran = true;
+  if (!s->host_loop) {
+    optx_sorted::Graph* g = nullptr;
+    OPTX_TRY(sorted_graph(s, P, a, &g));
+    OPTX_CUDA(cudaGraphLaunch(g->exec, st));
+  } else {
+    OPTX_CUDA(DISPATCH(s->math, launch_sorted_prep, a, s->d_ctrl, st));
+    for (;;) {  // the kernel's own watchdog ends a run that does not finish
+      for (int k = 0; k < 8; ++k)
+        OPTX_CUDA(DISPATCH(s->math, launch_sorted, s->minb, P, a, s->d_ctrl, s->grid, kSortBlock, st));
+      unsigned active = 0;
+      OPTX_CUDA(cudaMemcpyAsync(&active, &s->d_ctrl->active, sizeof(active), cudaMemcpyDeviceToHost, st));
+      OPTX_CUDA(cudaStreamSynchronize(st));
+      if (!active) break;
+    }
+  }
+  OPTX_CUDA(cudaEventRecord(s->ev1, st));
+  return OPTX_OK;
+}
+
+int optx_sorted_stats(optx_sorted* s, optx_sorted_counters* out, void* stream) {
+  if (s == nullptr || out == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = optx_sorted_counters{};
+  if (!s->ran) return OPTX_OK;
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  SortCtrl c{};
+  OPTX_CUDA(cudaMemcpyAsync(&c, s->d_ctrl, sizeof(c), cudaMemcpyDeviceToHost, st));
+  OPTX_CUDA(cudaStreamSynchronize(st));
+  OPTX_CUDA(cudaEventSynchronize(s->ev1));
+  float ms = 0.0f;
+  OPTX_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+  out->iterations = c.iter;
+  for (uint32_t q = 0; q < kSortQueues; ++q) out->queued[q] = c.queued[q];
+  out->drained = c.drained;
+  out->kernel_ms = ms;
+  if (c.error & kErrQueue) return fail(OPTX_ERR_CAPACITY, "sorted run: state queue overflow");
+  if (c.error & kErrWatchdog) return fail(OPTX_ERR_WATCHDOG, "sorted run: iteration cap reached");
+  return OPTX_OK;
+}
+
+}  // extern "C"
+
+// =============================================================================
 // Wavefront tally without device allocation.
 //
 // For callers that cannot call cudaMalloc: code running where another runtime

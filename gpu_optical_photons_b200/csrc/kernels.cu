@@ -739,6 +739,293 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
   }
 }
 
+// ---------------------------------------------------------------------------
+// Per-interaction sorted run: photons between steps wait in the state queue of
+// their pending interaction (Rayleigh scatter, a polished face, a painted face);
+// one launch per iteration. The launch's work items are the three input queues
+// and the iteration's fresh emissions, each segment padded to a multiple of 32,
+// so every warp takes 32 photons of one kind: step_act runs warp-uniform (the
+// Philox advance once per warp step), then step_move takes each survivor to its
+// next interaction and a warp-aggregated append (ballot + one atomic per queue)
+// writes it, 5 x 128-bit stores, into that queue of the other parity. Absorption,
+// black faces and the step limit end a photon at the move. The last block to
+// finish sets up the next iteration: the output queues become the input, fresh
+// photons fill the freed slots, and once nothing is left to emit and fewer than
+// `drain_below` photons are in flight, one last launch runs every remaining photon
+// to its end in place (the fused loop). Records depend only on (seed, photon id),
+// so they equal the history kernel's bit for bit.
+
+__device__ __forceinline__ float4 __uint_as_float4(uint4 v) {
+  return make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z),
+                     __uint_as_float(v.w));
+}
+
+// Offset, in float4, of word group g of queue slot `slot` (tiles of 32 photons).
+__device__ __forceinline__ size_t sort_off(uint32_t slot, uint32_t g) {
+  return ((static_cast<size_t>(slot >> 5) * kSortVec4 + g) << 5) + (slot & 31u);
+}
+
+__global__ void sorted_prep_kernel(const SortArgs A, SortCtrl* __restrict__ ctrl) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (uint32_t p = 0; p < 2u; ++p)
+    for (uint32_t q = 0; q < kSortQueues; ++q) ctrl->count[p][q].v = 0u;
+  const unsigned long long emit = A.n < A.cap ? A.n : A.cap;
+  ctrl->parity = 0u;
+  ctrl->emit_base = 0ull;
+  ctrl->emit_count = static_cast<unsigned>(emit);
+  ctrl->drain = (emit == A.n && emit < A.drain_below) ? 1u : 0u;
+  ctrl->blocks_done = 0u;
+  ctrl->iter = 0u;
+  ctrl->error = 0u;
+  ctrl->active = A.n > 0ull ? 1u : 0u;
+  for (uint32_t q = 0; q < kSortQueues; ++q) ctrl->queued[q] = 0ull;
+  ctrl->drained = 0ull;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// Waits until at most one group (the newest) of this thread's copies is pending.
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <int MINB>
+__global__ void __launch_bounds__(kSortThreads, MINB)
+    sorted_kernel(const DevParams P, const SortArgs A, SortCtrl* __restrict__ ctrl) {
+  // Host-loop launches past the end of the run do nothing (the flag only changes
+  // in the last block of a launch, after every block has read it).
+  if (ctrl->active == 0u) return;
+  // Per-warp double buffer: the warp's next 32 queued photons are copied here
+  // (cp.async, each lane its own slot) while it works on the current ones.
+  __shared__ __align__(16) uint4 s_stage[kSortThreads / 32][2][kSortVec4][32];
+  __shared__ uint32_t s_rel[kSortThreads / 32][2][32];
+  __shared__ unsigned long long s_cnt[7];  // 5 fates, sum nb, sum ns
+  if (threadIdx.x < 7u) s_cnt[threadIdx.x] = 0ull;
+  __syncthreads();
+
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t par = ctrl->parity, npar = par ^ 1u;
+  const bool drain = ctrl->drain != 0u;
+  const uint32_t c0 = ctrl->count[par][0].v, c1 = ctrl->count[par][1].v, c2 = ctrl->count[par][2].v;
+  const uint32_t ce = ctrl->emit_count;
+  const unsigned long long emit_base = ctrl->emit_base;
+  const uint32_t e1 = (c0 + 31u) & ~31u, e2 = e1 + ((c1 + 31u) & ~31u),
+                 e3 = e2 + ((c2 + 31u) & ~31u), e4 = e3 + ((ce + 31u) & ~31u);
+  const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long* const tally = A.tally;
+  const TallyDev tc = A.tc;
+
+  const uint32_t warp = threadIdx.x >> 5;
+  const uint32_t stride = n_warps << 5;
+  // Issues the copies of the queued photons at work item b into buffer `buf`
+  // (emissions and items past the end copy nothing); one commit group per call.
+  auto prefetch = [&](uint32_t b, uint32_t buf) {
+    if (b < e3) {
+      const uint32_t sg = b < e1 ? 0u : (b < e2 ? 1u : 2u);
+      const uint32_t i = b - (sg == 0u ? 0u : (sg == 1u ? e1 : e2)) + lane;
+      if (i < (sg == 0u ? c0 : (sg == 1u ? c1 : c2))) {
+        const uint4* q = reinterpret_cast<const uint4*>(A.q[par][sg]);
+#pragma unroll
+        for (uint32_t g = 0; g < kSortVec4; ++g) cp_async16(&s_stage[warp][buf][g][lane], q + sort_off(i, g));
+        cp_async4(&s_rel[warp][buf][lane], A.qid[par][sg] + i);
+      }
+    }
+    cp_async_commit();
+  };
+
+  uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0, snb = 0, sns = 0;
+  uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) << 5;
+  prefetch(base, 0u);
+  for (uint32_t k = 0; base < e4; base += stride, ++k) {
+    const uint32_t buf = k & 1u;
+    prefetch(base + stride, buf ^ 1u);
+    cp_async_wait_prev();  // this item's copies have landed
+    // The warp's segment: queue 0, 1, 2, or 3 = fresh emissions (warp-uniform).
+    const uint32_t seg = base < e1 ? 0u : (base < e2 ? 1u : (base < e3 ? 2u : 3u));
+    const uint32_t start = seg == 0u ? 0u : (seg == 1u ? e1 : (seg == 2u ? e2 : e3));
+    const uint32_t cnt = seg == 0u ? c0 : (seg == 1u ? c1 : (seg == 2u ? c2 : ce));
+    const uint32_t idx = base - start + lane;
+    const bool valid = idx < cnt;
+
+    Photon s;
+    Rng r;
+    ScoreAux aux{0u, 0.0f};
+    uint32_t rel = 0u, fate = kMaxSteps;
+    int hit = 0;
+    bool live = valid;
+    if (valid) {
+      if (seg < 3u) {
+        const float4 v0 = __uint_as_float4(s_stage[warp][buf][0][lane]);
+        const float4 v1 = __uint_as_float4(s_stage[warp][buf][1][lane]);
+        const uint4 v2 = s_stage[warp][buf][2][lane], v3 = s_stage[warp][buf][3][lane],
+                    v4 = s_stage[warp][buf][4][lane];
+        rel = s_rel[warp][buf][lane];
+        s.px = v0.x; s.py = v0.y; s.pz = v0.z; s.t = v0.w;
+        s.dx = v1.x; s.dy = v1.y; s.dz = v1.z; s.path = v1.w;
+        r.w[0] = v2.x; r.w[1] = v2.y; r.w[2] = v2.z; r.w[3] = v2.w;
+        r.w[4] = v3.x; r.w[5] = v3.y; r.w[6] = v3.z; r.w[7] = v3.w;
+        s.nb = v4.x; s.ns = v4.y;
+        r.o = v4.z & 0xffu;
+        hit = static_cast<int>(v4.z >> 8);
+        r.blk = v4.w;
+      } else {
+        rel = static_cast<uint32_t>(emit_base + idx);
+        r.init(A.first_id + rel, P.key_lo, P.key_hi, 0u);
+        start_photon<false>(P, s, r, A.first_id + rel, aux);
+      }
+    }
+    const uint64_t id = A.first_id + rel;
+    if (seg < 3u) {
+      const uint32_t m = __ballot_sync(kFull, valid);
+      if (valid) live = step_act<false>(P, s, r, id, fate, aux, hit, m);
+    }
+
+    int next = -1;
+    if (drain) {
+      // Last launch: the rest of each history in place (transport.hpp:151-159).
+      while (live) {
+        if (s.nb + s.ns >= P.max_steps) { fate = kMaxSteps; live = false; break; }
+        live = step_photon<false>(P, s, r, id, fate, aux);
+      }
+    } else if (live) {
+      // Photons that have made max_steps steps end here (each live step counted
+      // one boundary or one scatter).
+      if (s.nb + s.ns >= P.max_steps) {
+        fate = kMaxSteps;
+        live = false;
+      } else {
+        hit = step_move(P, s, r);
+        if (hit == kHitAbsorb) {  // bulk absorption (transport.hpp:98-101)
+          fate = kAbsorbedBulk;
+          live = false;
+        } else if (hit == kHitScatter) {
+          next = kQScatter;
+        } else {
+          const uint32_t model = face_model(P, hit);
+          if (model == kBlack) {  // black face: absorbed, no draw (transport.hpp:129-132)
+            ++s.nb;
+            fate = kAbsorbedSurface;
+            live = false;
+          } else {
+            next = model == kPolished ? kQFresnel : kQPainted;
+          }
+        }
+      }
+    }
+
+    // Survivors: warp-aggregated appends to the queue of their next interaction.
+#pragma unroll
+    for (uint32_t qq = 0; qq < kSortQueues; ++qq) {
+      const uint32_t m = __ballot_sync(kFull, next == static_cast<int>(qq));
+      if (m == 0u) continue;
+      uint32_t slot0 = 0u;
+      if (lane == static_cast<uint32_t>(__ffs(m) - 1))
+        slot0 = atomicAdd(&ctrl->count[npar][qq].v, static_cast<unsigned>(__popc(m)));
+      slot0 = __shfl_sync(kFull, slot0, __ffs(m) - 1);
+      if (next == static_cast<int>(qq)) {
+        const uint32_t slot = slot0 + __popc(m & lt);
+        if (slot < A.cap) {
+          float4* q = A.q[npar][qq];
+          uint4* qu = reinterpret_cast<uint4*>(q);
+          q[sort_off(slot, 0u)] = make_float4(s.px, s.py, s.pz, s.t);
+          q[sort_off(slot, 1u)] = make_float4(s.dx, s.dy, s.dz, s.path);
+          qu[sort_off(slot, 2u)] = make_uint4(r.w[0], r.w[1], r.w[2], r.w[3]);
+          qu[sort_off(slot, 3u)] = make_uint4(r.w[4], r.w[5], r.w[6], r.w[7]);
+          qu[sort_off(slot, 4u)] = make_uint4(s.nb, s.ns, r.o | (static_cast<uint32_t>(hit) << 8), r.blk);
+          A.qid[npar][qq][slot] = rel;
+        } else {
+          atomicOr(&ctrl->error, kErrQueue);
+        }
+      }
+    }
+
+    // Finished photons: record and tally.
+    if (valid && !live) {
+      if (A.rec.fate != nullptr) store_record(A.rec, rel, s, fate);
+      f0 += fate == 0u;
+      f1 += fate == 1u;
+      f2 += fate == 2u;
+      f3 += fate == 3u;
+      f4 += fate == 4u;
+      snb += s.nb;
+      sns += s.ns;
+      if (fate == kDetected && tally != nullptr) {
+        atomicAdd(tally + 5u + time_bin(s.t, tc.tscale, tc.time_bins), 1ull);
+        atomicAdd(tally + 6u + tc.time_bins + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins), 1ull);
+      }
+    }
+  }
+
+  // Fates and step sums: warp reductions, shared atomics, one global atomic per
+  // block and counter.
+  const uint32_t r0 = __reduce_add_sync(kFull, f0), r1 = __reduce_add_sync(kFull, f1),
+                 r2 = __reduce_add_sync(kFull, f2), r3 = __reduce_add_sync(kFull, f3),
+                 r4 = __reduce_add_sync(kFull, f4);
+  const unsigned long long rb = warp_sum_u64(snb), rs = warp_sum_u64(sns);
+  if (lane == 0u && tally != nullptr) {
+    if (r0) atomicAdd(&s_cnt[0], static_cast<unsigned long long>(r0));
+    if (r1) atomicAdd(&s_cnt[1], static_cast<unsigned long long>(r1));
+    if (r2) atomicAdd(&s_cnt[2], static_cast<unsigned long long>(r2));
+    if (r3) atomicAdd(&s_cnt[3], static_cast<unsigned long long>(r3));
+    if (r4) atomicAdd(&s_cnt[4], static_cast<unsigned long long>(r4));
+    if (rb) atomicAdd(&s_cnt[5], rb);
+    if (rs) atomicAdd(&s_cnt[6], rs);
+  }
+  __syncthreads();
+  if (threadIdx.x < 7u && tally != nullptr && s_cnt[threadIdx.x] != 0ull) {
+    const uint32_t at = threadIdx.x < 5u ? threadIdx.x : tc.len - 7u + threadIdx.x;
+    atomicAdd(tally + at, s_cnt[threadIdx.x]);
+  }
+
+  // ---- the last block to finish sets up the next iteration ----------------------
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned done = atomicAdd(&ctrl->blocks_done, 1u);
+    if (done == gridDim.x - 1u) {
+      __threadfence();
+      volatile SortCtrl* vc = ctrl;
+      unsigned long long live = 0ull;
+      for (uint32_t q = 0; q < kSortQueues; ++q) {
+        unsigned int k = vc->count[npar][q].v;
+        if (k > A.cap) k = A.cap;  // appends past cap were not written (error set)
+        vc->count[npar][q].v = k;
+        vc->queued[q] = vc->queued[q] + k;
+        vc->count[par][q].v = 0u;
+        live += k;
+      }
+      if (vc->drain) vc->drained = vc->drained + (static_cast<unsigned long long>(c0) + c1 + c2 + ce);
+      const unsigned long long next = vc->emit_base + vc->emit_count;
+      const unsigned long long remaining = A.n - next;
+      const unsigned long long room = A.cap > live ? A.cap - live : 0ull;
+      const unsigned long long emit = remaining < room ? remaining : room;
+      vc->emit_base = next;
+      vc->emit_count = static_cast<unsigned>(emit);
+      vc->parity = npar;
+      vc->drain = (emit == remaining && live + emit < A.drain_below) ? 1u : 0u;
+      vc->iter = vc->iter + 1u;
+      vc->blocks_done = 0u;
+      bool more = live + emit > 0ull && vc->error == 0u;
+      if (more && vc->iter >= A.iter_cap) {
+        vc->error = vc->error | kErrWatchdog;
+        more = false;
+      }
+      vc->active = more ? 1u : 0u;
+      __threadfence();
+      if (!more && A.use_graph != 0u) cudaGraphSetConditional(A.graph_handle, 0u);
+    }
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -827,6 +1114,35 @@ cudaError_t launch_wave(int mode, int batch, int minb, const DevParams& P, const
                         WaveCtrl* ctrl, int grid, int block, size_t smem, cudaStream_t st) {
   void* args[] = {const_cast<DevParams*>(&P), &A_dev, &ctrl};
   return cudaLaunchKernel(wave_kernel_fn(mode, batch, minb), dim3(grid), dim3(block), args, smem, st);
+}
+
+const void* sorted_prep_fn() { return reinterpret_cast<const void*>(&sorted_prep_kernel); }
+const void* sorted_kernel_fn(int minb) {
+  return minb == 3 ? reinterpret_cast<const void*>(&sorted_kernel<3>)
+                   : reinterpret_cast<const void*>(&sorted_kernel<4>);
+}
+
+cudaError_t launch_sorted(int minb, const DevParams& P, const SortArgs& A, SortCtrl* ctrl, int grid,
+                          int block, cudaStream_t st) {
+  void* args[] = {const_cast<DevParams*>(&P), const_cast<SortArgs*>(&A), &ctrl};
+  return cudaLaunchKernel(sorted_kernel_fn(minb), dim3(grid), dim3(block), args, 0, st);
+}
+
+cudaError_t launch_sorted_prep(const SortArgs& A, SortCtrl* ctrl, cudaStream_t st) {
+  sorted_prep_kernel<<<1, 32, 0, st>>>(A, ctrl);
+  return cudaGetLastError();
+}
+
+int sorted_blocks_per_sm(int minb, int block) {
+  // 42 KB of staging per block: ask for the largest shared-memory carve-out so
+  // that three or four blocks fit on an SM.
+  const void* fn = sorted_kernel_fn(minb);
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+    return 0;
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, block, 0) != cudaSuccess) return 0;
+  return b < minb ? b : minb;
 }
 
 cudaError_t launch_event_table(const unsigned long long* offsets, uint32_t n_events,

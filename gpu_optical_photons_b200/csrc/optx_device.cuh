@@ -322,18 +322,15 @@ __device__ __forceinline__ void start_photon(const DevParams& P, Photon& s, Rng&
   r.advance(k, id, P.key_lo, P.key_hi);
 }
 
-// One step (transport.hpp:71-145). Returns true while the photon is alive;
-// otherwise `fate` is set and the photon sits at its final interaction.
-// The window is advanced only for photons that stay alive.
-// One exit: every outcome falls through to the shared tail (rotation, flip,
-// window advance). With sync_mask != 0 (the lanes of the warp that call this
-// step together) the warp reconverges before the advance, so the Philox block
-// runs once per warp step for all lanes that need one rather than once per
-// divergent group.
-template <bool AUX>
-__device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& r, uint64_t id,
-                                            uint32_t& fate, ScoreAux& aux,
-                                            uint32_t sync_mask = 0u) {
+// A step's interaction, decided by step_move: a face index 0..5 (a boundary
+// hit), kHitScatter or kHitAbsorb.
+constexpr int kHitScatter = 6;
+constexpr int kHitAbsorb = 7;
+
+// First half of a step (transport.hpp:71-97): the exponential absorption and
+// scattering distances (window words 0 and 1), the box exit, and the move to the
+// nearest of the three. Returns the interaction; the window is not advanced.
+__device__ __forceinline__ int step_move(const DevParams& P, Photon& s, const Rng& r) {
   const float u_abs = r.uniform<0>(), u_sca = r.uniform<1>();
   const float s_abs = (P.abs_length == kInf) ? kInf : -P.abs_length * m_log(u_abs);
   const float s_sca = (P.scat_length == kInf) ? kInf : -P.scat_length * m_log(u_sca);
@@ -363,9 +360,8 @@ __device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& 
   const bool scatter = !absorb && s_sca < dist;
   const float d = absorb ? s_abs : (scatter ? s_sca : dist);
   float nx = s.px + d * s.dx, ny = s.py + d * s.dy, nz = s.pz + d * s.dz;
-  const int axis = face >> 1;
-  const bool boundary = !absorb && !scatter;
-  if (boundary) {  // snap onto the face plane, clamp in-plane (geometry.hpp:57-63)
+  if (!absorb && !scatter) {  // snap onto the face plane, clamp in-plane (geometry.hpp:57-63)
+    const int axis = face >> 1;
     const float sg = (face & 1) ? 1.0f : -1.0f;
     nx = (axis == 0) ? sg * P.hx : fminf(fmaxf(nx, -P.hx), P.hx);
     ny = (axis == 1) ? sg * P.hy : fminf(fmaxf(ny, -P.hy), P.hy);
@@ -376,14 +372,37 @@ __device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& 
   s.pz = nz;
   s.t = s.t + d * P.inv_speed;
   s.path = s.path + d;
+  return absorb ? kHitAbsorb : (scatter ? kHitScatter : face);
+}
 
+// Surface model of face `face` (the readout face is always polished).
+__device__ __forceinline__ uint32_t face_model(const DevParams& P, int face) {
+  return (face == kReadoutFace) ? kPolished : ((P.surf_bits >> (2 * face)) & 3u);
+}
+
+// Second half of a step (transport.hpp:98-145): the interaction `hit` at the
+// photon's position, then the window advance past the words the step used.
+// Returns true while the photon is alive; otherwise `fate` is set and the photon
+// sits at its final interaction. The window is advanced only for photons that
+// stay alive.
+// One exit: every outcome falls through to the shared tail (rotation, flip,
+// window advance). With sync_mask != 0 (the lanes of the warp that call this
+// step together) the warp reconverges before the advance, so the Philox block
+// runs once per warp step for all lanes that need one rather than once per
+// divergent group.
+template <bool AUX>
+__device__ __forceinline__ bool step_act(const DevParams& P, Photon& s, Rng& r, uint64_t id,
+                                         uint32_t& fate, ScoreAux& aux, int hit,
+                                         uint32_t sync_mask = 0u) {
+  const int face = hit;
+  const int axis = face >> 1;
   uint32_t k = 2u;           // words consumed by this step
   bool live = true, rotate = false, flip = false;
   float ax = s.dx, ay = s.dy, az = s.dz, ct = 0.0f, phi_u = 0.0f;
-  if (absorb) {
+  if (hit == kHitAbsorb) {
     fate = kAbsorbedBulk;
     live = false;
-  } else if (scatter) {
+  } else if (hit == kHitScatter) {
     ++s.ns;
     ct = rayleigh_cos(r.uniform<2>());
     phi_u = r.uniform<3>();
@@ -392,7 +411,7 @@ __device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& 
   } else {
     ++s.nb;
     const float cos_i = fabsf(axis == 0 ? s.dx : (axis == 1 ? s.dy : s.dz));
-    const uint32_t model = (face == kReadoutFace) ? kPolished : ((P.surf_bits >> (2 * face)) & 3u);
+    const uint32_t model = face_model(P, face);
     if (model == kPolished) {
       // Readout face: interface to n_det, transmitted = detected; other faces:
       // interface to n_out, transmitted = escaped (transport.hpp:108-128).
@@ -442,6 +461,15 @@ __device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& 
   if (sync_mask != 0u) __syncwarp(sync_mask);
   if (live) r.advance(k, id, P.key_lo, P.key_hi);
   return live;
+}
+
+// One step (transport.hpp:71-145): move, then interact.
+template <bool AUX>
+__device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& r, uint64_t id,
+                                            uint32_t& fate, ScoreAux& aux,
+                                            uint32_t sync_mask = 0u) {
+  const int hit = step_move(P, s, r);
+  return step_act<AUX>(P, s, r, id, fate, aux, hit, sync_mask);
 }
 
 // Tally binning (transport.hpp:170-181); tscale = time_bins / time_max in float.

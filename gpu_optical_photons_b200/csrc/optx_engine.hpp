@@ -106,6 +106,56 @@ inline __host__ __device__ uint32_t moment_smem_bytes(uint32_t time_bins) {
   return b <= kMomentSmemMaxBytes ? b : 0u;
 }
 
+// Per-interaction sorted run (sorted_kernel): between steps each photon waits in
+// the state queue of its pending interaction; every iteration is one launch in
+// which each warp takes 32 photons of one queue (or 32 fresh emissions), so the
+// interaction code runs warp-uniform, and appends the survivors, moved to their
+// next interaction, to the queues of the other parity.
+enum SortQueue : uint32_t { kQScatter = 0, kQFresnel = 1, kQPainted = 2, kSortQueues = 3 };
+// A queued photon: 5 x 16 B in tiles of 32 photons (px py pz t | dx dy dz path |
+// window words 0-3 | words 4-7 | nb ns o+hit blk), plus its relative index.
+constexpr uint32_t kSortVec4 = 5u;
+constexpr int kSortThreads = 256;  // threads per block of sorted_kernel
+constexpr uint32_t kSortBytesPerPhoton = kSortVec4 * 16u + 4u;
+
+// Passed by value (kernel parameter: read through the constant bank).
+struct SortArgs {
+  float4* q[2][kSortQueues];            // [parity][queue] tiles
+  uint32_t* qid[2][kSortQueues];        // relative photon index per slot
+  uint32_t cap;                         // slots per queue = photons in flight (multiple of 32)
+  uint32_t drain_below;                 // finish every photon in one launch once fewer are left
+  unsigned long long n;                 // photons in the run
+  unsigned long long first_id;          // Philox id of relative photon 0
+  unsigned long long* tally;            // null: no tally (else ADDED to, flat layout)
+  TallyDev tc;
+  DevRecords rec;                       // rec.fate null: no records
+  unsigned long long graph_handle;      // cudaGraphConditionalHandle of the iteration loop
+  uint32_t iter_cap;                    // watchdog: max iterations per run
+  uint32_t use_graph;                   // 1: iterations run as a graph while node (set its condition)
+};
+
+// A queue's append counter, alone in its 128-byte line: every warp of a launch
+// adds to it, so the three queues' counters should not share an L2 sector.
+struct alignas(128) SortCounter {
+  unsigned int v;
+  unsigned int pad[31];
+};
+
+struct SortCtrl {
+  SortCounter count[2][kSortQueues];    // photons per queue [parity] (appends are atomic)
+  unsigned int parity;                  // parity of this iteration's input queues
+  unsigned int emit_count;              // fresh photons this iteration
+  unsigned long long emit_base;         // relative index of the first of them
+  unsigned int drain;                   // 1: this iteration runs every photon to its end
+  unsigned int blocks_done;             // blocks finished (atomic)
+  unsigned int iter;                    // iterations run
+  unsigned int error;                   // kErrQueue, kErrWatchdog
+  unsigned int active;                  // 0 once the run is complete (launches return at once)
+  unsigned long long queued[kSortQueues];  // photons that went through each queue
+  unsigned long long drained;           // photons finished by the drain launch
+};
+static_assert(sizeof(SortCtrl) <= 1024, "sorted control block");
+
 #define OPTX_DECLARE_LAUNCHERS(NS)                                                               \
   namespace NS {                                                                                 \
   cudaError_t launch_history_records(const DevParams& P, uint64_t first_id, uint64_t n,          \
@@ -128,6 +178,14 @@ inline __host__ __device__ uint32_t moment_smem_bytes(uint32_t time_bins) {
   cudaError_t launch_event_table(const unsigned long long* offsets, uint32_t n_events,           \
                                  uint32_t* table, unsigned long long total, uint32_t shift,      \
                                  cudaStream_t st);                                               \
+  /* Per-interaction sorted run: prep (one thread) and one iteration. */                         \
+  /* minb: 3 or 4 resident blocks per SM (the register budget) */                               \
+  const void* sorted_prep_fn();                                                                  \
+  const void* sorted_kernel_fn(int minb);                                                        \
+  int sorted_blocks_per_sm(int minb, int block);                                                 \
+  cudaError_t launch_sorted(int minb, const DevParams& P, const SortArgs& A, SortCtrl* ctrl,      \
+                            int grid, int block, cudaStream_t st);                               \
+  cudaError_t launch_sorted_prep(const SortArgs& A, SortCtrl* ctrl, cudaStream_t st);            \
   }
 
 OPTX_DECLARE_LAUNCHERS(fast)

@@ -193,6 +193,56 @@ class WavefrontEngine:
         return out, st.as_dict(), tm.as_dict()
 
 
+class SortedEngine:
+    """Per-interaction sorted kernels (optx_sorted_*): photons wait between steps
+    in state queues sorted by their pending interaction (Rayleigh scatter,
+    polished face, painted face); every launch gives each warp 32 photons of one
+    kind. Same records as `records_device` bit for bit, same tallies as
+    `tally_device`; one configuration per run, asynchronous on the stream."""
+
+    def __init__(self, capacity: int = 0, drain_below: int = 0, math="fast", host_loop: bool = False,
+                 blocks_per_sm: int = 0):
+        from .backend import _math
+        self._h = ctypes.c_void_p()
+        cfg = _lib.CSortedConfig(capacity, drain_below, _math(math), blocks_per_sm, 1 if host_loop else 0)
+        _lib.call("optx_sorted_create", ctypes.byref(cfg), ctypes.byref(self._h))
+
+    def close(self):
+        if self._h:
+            _lib.lib().optx_sorted_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, p: SimParams, n: int, first_id: int = 0, tally: TallyConfig | None = None,
+            tally_out=None, records_out=None, stream=None):
+        """Runs n photons. With `tally` set, ADDS into `tally_out` (a torch int64
+        device tensor of tally.length; a zeroed one is made when None). Records
+        go into `records_out` (a dict from backend.device_records) when given.
+        Returns (tally_out, records_out)."""
+        import torch
+        if tally is not None and tally_out is None:
+            tally_out = torch.zeros(tally.length, dtype=torch.int64, device="cuda")
+        cp, cf = _lib.params_args(p)
+        cc = tally.to_c() if tally is not None else None
+        cr = _crec_from_torch(records_out) if records_out is not None else None
+        _lib.call("optx_sorted_run", self._h, ctypes.byref(cp), _lib.ref(cf),
+                  ctypes.byref(cc) if cc is not None else None, n, first_id,
+                  ctypes.c_void_p(tally_out.data_ptr()) if tally is not None else None,
+                  ctypes.byref(cr) if cr is not None else None, _stream_ptr(stream))
+        return tally_out, records_out
+
+    def stats(self, stream=None) -> dict:
+        """Counters of the last run (synchronises the stream)."""
+        st = _lib.CSortedCounters()
+        _lib.call("optx_sorted_stats", self._h, ctypes.byref(st), _stream_ptr(stream))
+        return st.as_dict()
+
+
 def wavefront_tally(p: SimParams, c: TallyConfig, n: int, first_id: int = 0,
                     config: WaveConfig | None = None):
     """Single-configuration tally through the wavefront engine. Returns (Tally, flat, stats)."""

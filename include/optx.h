@@ -180,6 +180,50 @@ int optx_tally_device(const optx_params* p, const optx_faces* faces, const optx_
                       uint64_t n, uint64_t first_id, uint64_t* dev_tally, int block_size, int math,
                       void* stream);
 
+/* ---- per-interaction sorted kernels (extension) -------------------------
+ * The design the reference's profiling notes name as the next step after the
+ * fused event kernel (PROFILING.md:136-143, README.md:719-720): between steps
+ * each photon waits in an HBM state queue for its pending interaction (Rayleigh
+ * scatter, a polished face, a painted face), and each warp of an iteration's
+ * launch takes 32 photons of one kind, so the interaction code runs without
+ * divergence between kinds. One configuration per run; the records equal the
+ * history kernel's (optx_records_device) bit for bit, and the tallies
+ * optx_tally_device's. */
+typedef struct optx_sorted optx_sorted;
+typedef struct optx_sorted_counters {
+  uint64_t iterations; /* launches of the last run (one per iteration) */
+  uint64_t queued[3];  /* photons that went through the scatter, polished-face and
+                          painted-face queues */
+  uint64_t drained;    /* photons finished by the run's last, in-place launch */
+  double kernel_ms;    /* device time of the last run */
+} optx_sorted_counters;
+/* Sorted-run configuration. Zero fields take defaults. */
+typedef struct optx_sorted_config {
+  uint32_t capacity;      /* photons in flight = slots per queue, rounded up to 32 (default 2^21);
+                             the queues take 2 x 3 x 84 bytes per slot */
+  uint32_t drain_below;   /* once nothing is left to emit and fewer photons than this are in
+                             flight, one last launch runs each of them to its end (default: the
+                             number of resident threads) */
+  int32_t math;           /* OPTX_MATH_FAST / OPTX_MATH_EXACT / OPTX_MATH_APPROX */
+  int32_t blocks_per_sm;  /* register budget: 3 (80 registers, default) or 4 (64) blocks of 256 */
+  uint32_t host_loop;     /* 1: iterations launched from the host (one stream synchronisation per
+                             8; optx_sorted_run is then synchronous) instead of a CUDA-graph
+                             while loop, for profilers that do not see kernels inside
+                             conditional graph nodes */
+} optx_sorted_config;
+int optx_sorted_create(const optx_sorted_config* cfg, optx_sorted** out);
+int optx_sorted_destroy(optx_sorted* s);
+/* n photons (ids first_id ..) of one configuration, async on `stream`: ADDS the
+ * tally into dev_tally (flat layout as optx_run_tally; NULL = none) and writes
+ * dev_records (n entries; NULL = none). n < 2^32. Run errors are reported by
+ * the next optx_sorted_stats. */
+int optx_sorted_run(optx_sorted* s, const optx_params* p, const optx_faces* faces,
+                    const optx_tally_config* c, uint64_t n, uint64_t first_id,
+                    uint64_t* dev_tally, const optx_records* dev_records, void* stream);
+/* Counters of the last run; synchronises `stream`. OPTX_ERR_CAPACITY or
+ * OPTX_ERR_WATCHDOG when the run failed. */
+int optx_sorted_stats(optx_sorted* s, optx_sorted_counters* stats, void* stream);
+
 /* ---- wavefront engine (extension: persistent, graph-captured, batched) -- */
 typedef struct optx_engine optx_engine;
 /* An engine for up to max_events events and max_photons photons per run. The

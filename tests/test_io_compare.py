@@ -184,6 +184,8 @@ def test_cli_records_out_against_reference_cpu(oracle, tmp_path):
     ["--config", "config3", "--engine", "wave", "--n", "2e5", "--bps", "7"],
     ["--config", "config1", "--engine", "wave", "--n", "2e5", "--cadence", "8", "--host-loop"],
     ["--engine", "gensteps", "--n", "16"],
+    ["--config", "config2", "--engine", "sorted", "--n", "2e5", "--capacity", "8192"],
+    ["--config", "config3", "--engine", "sorted", "--n", "2e5", "--host-loop", "--bps", "4"],
 ])
 def test_cli_engines_print_a_consistent_line(engine, capsys, tmp_path, argv):
     """Every engine of the command-line runner prints one JSON line whose fates
