@@ -1813,6 +1813,7 @@ constexpr int kSortBlock = kSortThreads;
 constexpr uint32_t kSortDefaultCap = 1u << 21;
 
 int sorted_free(optx_sorted* s) {
+  if (s->ran && s->ev1 != nullptr) cudaEventSynchronize(s->ev1);  // the last run no longer uses the queues
   for (auto& g : s->graphs) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
     if (g.graph) cudaGraphDestroy(g.graph);

@@ -227,6 +227,14 @@ class SortedEngine:
         import torch
         if tally is not None and tally_out is None:
             tally_out = torch.zeros(tally.length, dtype=torch.int64, device="cuda")
+        # The kernels write through raw pointers: check sizes and placement here.
+        if tally is not None and not (tally_out.is_cuda and tally_out.dtype == torch.int64
+                                      and tally_out.is_contiguous() and tally_out.numel() >= tally.length):
+            raise ValueError(f"tally_out must be a contiguous int64 CUDA tensor of >= {tally.length} entries")
+        if records_out is not None:
+            for k, v in records_out.items():
+                if not (v.is_cuda and v.is_contiguous() and v.numel() >= n):
+                    raise ValueError(f"records_out[{k!r}] must be a contiguous CUDA tensor of >= {n} entries")
         cp, cf = _lib.params_args(p)
         cc = tally.to_c() if tally is not None else None
         cr = _crec_from_torch(records_out) if records_out is not None else None

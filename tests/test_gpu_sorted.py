@@ -162,3 +162,19 @@ def test_host_loop_runs_the_same_iterations(engine):
         _lib.call("optx_sorted_create", ctypes.byref(_lib.CSortedConfig(0, 0, 0, 0, 2)), ctypes.byref(h))
     with pytest.raises(InvalidArgument):
         SortedEngine(blocks_per_sm=5)
+
+
+def test_output_buffers_are_checked_before_launch(engine):
+    import torch
+    p, c = P.config1()
+    eng = SortedEngine(4096)
+    with pytest.raises(ValueError):
+        eng.run(p, 1000, tally=c, tally_out=torch.zeros(c.length - 1, dtype=torch.int64, device="cuda"))
+    with pytest.raises(ValueError):
+        eng.run(p, 1000, tally=c, tally_out=torch.zeros(c.length, dtype=torch.int32, device="cuda"))
+    with pytest.raises(ValueError):
+        eng.run(p, 1000, records_out=device_records(999))
+    out, _ = eng.run(p, 1000, tally=c)  # the engine is untouched by the refusals
+    eng.stats()
+    eng.close()
+    assert int(out[:5].sum()) == 1000
