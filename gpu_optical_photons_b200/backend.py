@@ -157,6 +157,23 @@ def device_records(n: int, device="cuda"):
     return d
 
 
+def check_records_out(d, n: int) -> None:
+    """Device record arrays are written through raw pointers: each must be a
+    contiguous CUDA tensor of at least n entries of its record field's size."""
+    for k in Records.FIELDS:
+        v = d[k]
+        if not (v.is_cuda and v.is_contiguous() and v.numel() >= n
+                and v.element_size() == (1 if k == "fate" else 4)):
+            raise ValueError(f"records[{k!r}] must be a contiguous CUDA tensor of >= {n} "
+                             f"{'1' if k == 'fate' else '4'}-byte entries")
+
+
+def check_tally_out(t, length: int) -> None:
+    import torch
+    if not (t.is_cuda and t.dtype == torch.int64 and t.is_contiguous() and t.numel() >= length):
+        raise ValueError(f"tally must be a contiguous int64 CUDA tensor of >= {length} entries")
+
+
 def _crec_from_torch(d) -> _lib.CRecords:
     return _lib.CRecords(*[d[k].data_ptr() for k in Records.FIELDS])
 
@@ -165,6 +182,7 @@ def records_device(p: SimParams, n: int, first_id: int = 0, out=None, block_size
                    math="fast", stream=None):
     """History kernel into torch device arrays (asynchronous on the stream)."""
     out = device_records(n) if out is None else out
+    check_records_out(out, n)
     cp, cf = _lib.params_args(p)
     cr = _crec_from_torch(out)
     _lib.call("optx_records_device", ctypes.byref(cp), _lib.ref(cf), n, first_id, ctypes.byref(cr),
@@ -173,10 +191,14 @@ def records_device(p: SimParams, n: int, first_id: int = 0, out=None, block_size
 
 
 def tally_device(p: SimParams, c: TallyConfig, n: int, first_id: int = 0, out=None,
-                 block_size: int = 256, math="fast", stream=None):
-    """History tally kernel accumulating into a torch int64 device tensor of c.length."""
+                 block_size: int = 256, math="fast", stream=None, check: bool = True):
+    """History tally kernel accumulating into a torch int64 device tensor of
+    c.length. `check=False` skips the output check for callers that checked the
+    buffer once for many launches."""
     import torch
     out = torch.zeros(c.length, dtype=torch.int64, device="cuda") if out is None else out
+    if check:
+        check_tally_out(out, c.length)
     cp, cf = _lib.params_args(p)
     cc = c.to_c()
     _lib.call("optx_tally_device", ctypes.byref(cp), _lib.ref(cf), ctypes.byref(cc), n, first_id,

@@ -16,7 +16,7 @@ import numpy as np
 
 from . import _lib
 from .params import (CSimParams, CFaces, LAMBERTIAN, POINT, SimParams, TallyConfig)
-from .backend import Tally, _stream_ptr, _crec_from_torch
+from .backend import Tally, _stream_ptr, _crec_from_torch, check_records_out, check_tally_out
 
 
 @dataclass
@@ -157,6 +157,11 @@ class WavefrontEngine:
         _lib.call("optx_engine_run_tally", self._h, ctypes.c_void_p(stream or 0))
 
     def run_records(self, dev_records, stream=0):
+        """Per-photon records of the uploaded batch into device arrays (one entry
+        per photon, in batch order). Sizes are checked when the host knows the
+        batch's photon count (not after set_gensteps_device)."""
+        if self.counts is not None:
+            check_records_out(dev_records, int(np.asarray(self.counts, np.uint64).sum()))
         cr = _crec_from_torch(dev_records)
         _lib.call("optx_engine_run_records", self._h, ctypes.byref(cr), ctypes.c_void_p(stream or 0))
 
@@ -228,13 +233,10 @@ class SortedEngine:
         if tally is not None and tally_out is None:
             tally_out = torch.zeros(tally.length, dtype=torch.int64, device="cuda")
         # The kernels write through raw pointers: check sizes and placement here.
-        if tally is not None and not (tally_out.is_cuda and tally_out.dtype == torch.int64
-                                      and tally_out.is_contiguous() and tally_out.numel() >= tally.length):
-            raise ValueError(f"tally_out must be a contiguous int64 CUDA tensor of >= {tally.length} entries")
+        if tally is not None:
+            check_tally_out(tally_out, tally.length)
         if records_out is not None:
-            for k, v in records_out.items():
-                if not (v.is_cuda and v.is_contiguous() and v.numel() >= n):
-                    raise ValueError(f"records_out[{k!r}] must be a contiguous CUDA tensor of >= {n} entries")
+            check_records_out(records_out, n)
         cp, cf = _lib.params_args(p)
         cc = tally.to_c() if tally is not None else None
         cr = _crec_from_torch(records_out) if records_out is not None else None

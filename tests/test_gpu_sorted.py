@@ -178,3 +178,21 @@ def test_output_buffers_are_checked_before_launch(engine):
     eng.stats()
     eng.close()
     assert int(out[:5].sum()) == 1000
+
+
+def test_history_and_engine_wrappers_check_their_buffers(engine):
+    import torch
+    from gpu_optical_photons_b200.wavefront import WavefrontEngine
+    p, c = P.config1()
+    with pytest.raises(ValueError):
+        records_device(p, 100, out=device_records(99))
+    with pytest.raises(ValueError):
+        tally_device(p, c, 100, out=torch.zeros(c.length, dtype=torch.int64))  # host tensor
+    eng = WavefrontEngine(c, 1, 1000)
+    eng.set_events([p], [1000])
+    with pytest.raises(ValueError):
+        eng.run_records(device_records(999))
+    out = device_records(1000)
+    eng.run_records(out)
+    eng.close()
+    assert compare_histories(records_to_numpy(out), records_to_numpy(records_device(p, 1000)))["bitwise_identical"] == 1000
