@@ -1786,7 +1786,7 @@ int optx_run_records_event(const optx_params* p, const optx_faces* faces, uint64
 struct optx_sorted {
   std::mutex mu;
   int math = OPTX_MATH_FAST;
-  int minb = 3;  // resident blocks per SM (register budget)
+  int minb = 4;  // resident blocks per SM (register budget)
   uint32_t cap = 0, drain_below = 0;
   bool host_loop = false;
   int grid = 0;
@@ -1896,7 +1896,7 @@ int optx_sorted_create(const optx_sorted_config* cfg, optx_sorted** out) {
   const uint64_t cap = k.capacity == 0u ? kSortDefaultCap : ((uint64_t(k.capacity) + 31u) & ~uint64_t(31));
   if (cap > (1ull << 28)) return fail(OPTX_ERR_INVALID_ARGUMENT, "capacity must be <= 2^28 photons");
   OPTX_TRY(ensure_device());
-  const int minb = k.blocks_per_sm != 0 ? k.blocks_per_sm : 3;
+  const int minb = k.blocks_per_sm != 0 ? k.blocks_per_sm : 4;
   const int bps = DISPATCH(k.math, sorted_blocks_per_sm, minb, kSortBlock);
   if (bps <= 0) return fail(OPTX_ERR_RUNTIME, "sorted kernel cannot be resident");
   optx_sorted* s = new optx_sorted();

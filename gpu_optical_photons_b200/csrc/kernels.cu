@@ -782,32 +782,12 @@ __global__ void sorted_prep_kernel(const SortArgs A, SortCtrl* __restrict__ ctrl
   ctrl->drained = 0ull;
 }
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
-                   static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
-               "l"(gmem)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
-                   static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
-               "l"(gmem)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-// Waits until at most one group (the newest) of this thread's copies is pending.
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
 template <int MINB>
 __global__ void __launch_bounds__(kSortThreads, MINB)
     sorted_kernel(const DevParams P, const SortArgs A, SortCtrl* __restrict__ ctrl) {
   // Host-loop launches past the end of the run do nothing (the flag only changes
   // in the last block of a launch, after every block has read it).
   if (ctrl->active == 0u) return;
-  // Per-warp double buffer: the warp's next 32 queued photons are copied here
-  // (cp.async, each lane its own slot) while it works on the current ones.
-  __shared__ __align__(16) uint4 s_stage[kSortThreads / 32][2][kSortVec4][32];
-  __shared__ uint32_t s_rel[kSortThreads / 32][2][32];
   __shared__ unsigned long long s_cnt[7];  // 5 fates, sum nb, sum ns
   if (threadIdx.x < 7u) s_cnt[threadIdx.x] = 0ull;
   __syncthreads();
@@ -825,31 +805,11 @@ __global__ void __launch_bounds__(kSortThreads, MINB)
   unsigned long long* const tally = A.tally;
   const TallyDev tc = A.tc;
 
-  const uint32_t warp = threadIdx.x >> 5;
   const uint32_t stride = n_warps << 5;
-  // Issues the copies of the queued photons at work item b into buffer `buf`
-  // (emissions and items past the end copy nothing); one commit group per call.
-  auto prefetch = [&](uint32_t b, uint32_t buf) {
-    if (b < e3) {
-      const uint32_t sg = b < e1 ? 0u : (b < e2 ? 1u : 2u);
-      const uint32_t i = b - (sg == 0u ? 0u : (sg == 1u ? e1 : e2)) + lane;
-      if (i < (sg == 0u ? c0 : (sg == 1u ? c1 : c2))) {
-        const uint4* q = reinterpret_cast<const uint4*>(A.q[par][sg]);
-#pragma unroll
-        for (uint32_t g = 0; g < kSortVec4; ++g) cp_async16(&s_stage[warp][buf][g][lane], q + sort_off(i, g));
-        cp_async4(&s_rel[warp][buf][lane], A.qid[par][sg] + i);
-      }
-    }
-    cp_async_commit();
-  };
 
   uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0, snb = 0, sns = 0;
   uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) << 5;
-  prefetch(base, 0u);
-  for (uint32_t k = 0; base < e4; base += stride, ++k) {
-    const uint32_t buf = k & 1u;
-    prefetch(base + stride, buf ^ 1u);
-    cp_async_wait_prev();  // this item's copies have landed
+  for (; base < e4; base += stride) {
     // The warp's segment: queue 0, 1, 2, or 3 = fresh emissions (warp-uniform).
     const uint32_t seg = base < e1 ? 0u : (base < e2 ? 1u : (base < e3 ? 2u : 3u));
     const uint32_t start = seg == 0u ? 0u : (seg == 1u ? e1 : (seg == 2u ? e2 : e3));
@@ -865,11 +825,14 @@ __global__ void __launch_bounds__(kSortThreads, MINB)
     bool live = valid;
     if (valid) {
       if (seg < 3u) {
-        const float4 v0 = __uint_as_float4(s_stage[warp][buf][0][lane]);
-        const float4 v1 = __uint_as_float4(s_stage[warp][buf][1][lane]);
-        const uint4 v2 = s_stage[warp][buf][2][lane], v3 = s_stage[warp][buf][3][lane],
-                    v4 = s_stage[warp][buf][4][lane];
-        rel = s_rel[warp][buf][lane];
+        // The warp reads one whole tile: 5 coalesced 512-byte loads, streamed
+        // past L1 (each photon is read once per iteration).
+        const uint4* q = reinterpret_cast<const uint4*>(A.q[par][seg]);
+        const float4 v0 = __uint_as_float4(__ldcs(q + sort_off(idx, 0u)));
+        const float4 v1 = __uint_as_float4(__ldcs(q + sort_off(idx, 1u)));
+        const uint4 v2 = __ldcs(q + sort_off(idx, 2u)), v3 = __ldcs(q + sort_off(idx, 3u)),
+                    v4 = __ldcs(q + sort_off(idx, 4u));
+        rel = __ldcs(A.qid[par][seg] + idx);
         s.px = v0.x; s.py = v0.y; s.pz = v0.z; s.t = v0.w;
         s.dx = v1.x; s.dy = v1.y; s.dz = v1.z; s.path = v1.w;
         r.w[0] = v2.x; r.w[1] = v2.y; r.w[2] = v2.z; r.w[3] = v2.w;
@@ -1134,12 +1097,7 @@ cudaError_t launch_sorted_prep(const SortArgs& A, SortCtrl* ctrl, cudaStream_t s
 }
 
 int sorted_blocks_per_sm(int minb, int block) {
-  // 42 KB of staging per block: ask for the largest shared-memory carve-out so
-  // that three or four blocks fit on an SM.
   const void* fn = sorted_kernel_fn(minb);
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                           cudaSharedmemCarveoutMaxShared) != cudaSuccess)
-    return 0;
   int b = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, block, 0) != cudaSuccess) return 0;
   return b < minb ? b : minb;

@@ -205,7 +205,7 @@ typedef struct optx_sorted_config {
                              flight, one last launch runs each of them to its end (default: the
                              number of resident threads) */
   int32_t math;           /* OPTX_MATH_FAST / OPTX_MATH_EXACT / OPTX_MATH_APPROX */
-  int32_t blocks_per_sm;  /* register budget: 3 (80 registers, default) or 4 (64) blocks of 256 */
+  int32_t blocks_per_sm;  /* register budget: 4 (64 registers, default) or 3 (80) blocks of 256 */
   uint32_t host_loop;     /* 1: iterations launched from the host (one stream synchronisation per
                              8; optx_sorted_run is then synchronous) instead of a CUDA-graph
                              while loop, for profilers that do not see kernels inside
