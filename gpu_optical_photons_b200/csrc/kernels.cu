@@ -887,28 +887,32 @@ __global__ void __launch_bounds__(kSortThreads, MINB)
     }
 
     // Survivors: warp-aggregated appends to the queue of their next interaction.
-#pragma unroll
-    for (uint32_t qq = 0; qq < kSortQueues; ++qq) {
-      const uint32_t m = __ballot_sync(kFull, next == static_cast<int>(qq));
-      if (m == 0u) continue;
-      uint32_t slot0 = 0u;
-      if (lane == static_cast<uint32_t>(__ffs(m) - 1))
-        slot0 = atomicAdd(&ctrl->count[npar][qq].v, static_cast<unsigned>(__popc(m)));
-      slot0 = __shfl_sync(kFull, slot0, __ffs(m) - 1);
-      if (next == static_cast<int>(qq)) {
-        const uint32_t slot = slot0 + __popc(m & lt);
-        if (slot < A.cap) {
-          float4* q = A.q[npar][qq];
-          uint4* qu = reinterpret_cast<uint4*>(q);
-          q[sort_off(slot, 0u)] = make_float4(s.px, s.py, s.pz, s.t);
-          q[sort_off(slot, 1u)] = make_float4(s.dx, s.dy, s.dz, s.path);
-          qu[sort_off(slot, 2u)] = make_uint4(r.w[0], r.w[1], r.w[2], r.w[3]);
-          qu[sort_off(slot, 3u)] = make_uint4(r.w[4], r.w[5], r.w[6], r.w[7]);
-          qu[sort_off(slot, 4u)] = make_uint4(s.nb, s.ns, r.o | (static_cast<uint32_t>(hit) << 8), r.blk);
-          A.qid[npar][qq][slot] = rel;
-        } else {
-          atomicOr(&ctrl->error, kErrQueue);
-        }
+    // Lanes 0-2 reserve the warp's slots in the three queues with one atomic
+    // instruction (one round trip), then each survivor writes its state.
+    const uint32_t m0 = __ballot_sync(kFull, next == static_cast<int>(kQScatter)),
+                   m1 = __ballot_sync(kFull, next == static_cast<int>(kQFresnel)),
+                   m2 = __ballot_sync(kFull, next == static_cast<int>(kQPainted));
+    uint32_t base_q = 0u;
+    if (lane < kSortQueues) {
+      const uint32_t mq = lane == 0u ? m0 : (lane == 1u ? m1 : m2);
+      if (mq != 0u) base_q = atomicAdd(&ctrl->count[npar][lane].v, static_cast<unsigned>(__popc(mq)));
+    }
+    const uint32_t b0 = __shfl_sync(kFull, base_q, 0), b1 = __shfl_sync(kFull, base_q, 1),
+                   b2 = __shfl_sync(kFull, base_q, 2);
+    if (next >= 0) {
+      const uint32_t mq = next == 0 ? m0 : (next == 1 ? m1 : m2);
+      const uint32_t slot = (next == 0 ? b0 : (next == 1 ? b1 : b2)) + __popc(mq & lt);
+      if (slot < A.cap) {
+        float4* q = A.q[npar][next];
+        uint4* qu = reinterpret_cast<uint4*>(q);
+        q[sort_off(slot, 0u)] = make_float4(s.px, s.py, s.pz, s.t);
+        q[sort_off(slot, 1u)] = make_float4(s.dx, s.dy, s.dz, s.path);
+        qu[sort_off(slot, 2u)] = make_uint4(r.w[0], r.w[1], r.w[2], r.w[3]);
+        qu[sort_off(slot, 3u)] = make_uint4(r.w[4], r.w[5], r.w[6], r.w[7]);
+        qu[sort_off(slot, 4u)] = make_uint4(s.nb, s.ns, r.o | (static_cast<uint32_t>(hit) << 8), r.blk);
+        A.qid[npar][next][slot] = rel;
+      } else {
+        atomicOr(&ctrl->error, kErrQueue);
       }
     }
 
