@@ -59,6 +59,8 @@ def test_struct_layouts():
     assert ctypes.sizeof(_lib.CEventStats) == 40
     assert ctypes.sizeof(_lib.CWaveConfig) == 48
     assert ctypes.sizeof(_lib.CGenstep) == 40
+    assert ctypes.sizeof(_lib.CSortedConfig) == 20
+    assert ctypes.sizeof(_lib.CSortedCounters) == 48
 
 
 def test_invalid_arguments_raise_value_error(lib):
@@ -77,6 +79,27 @@ def test_invalid_arguments_raise_value_error(lib):
         g.run_gpu_records(P.SimParams(surface=7), 10)
     with pytest.raises(ValueError):
         g.run_gpu_records(P.SimParams(), 10, math=5)
+
+
+def test_sorted_run_rejects_invalid_arguments_before_any_device_call(lib):
+    """optx_sorted_*: bad configurations and NULL handles are refused on the host,
+    with or without a GPU."""
+    h = ctypes.c_void_p()
+    bad = [(0, 0, 5, 0, 0),              # math
+           (0, 0, 0, 5, 0),              # blocks_per_sm
+           (0, 0, 0, 0, 2),              # host_loop
+           ((1 << 28) + 64, 0, 0, 0, 0)]  # capacity
+    for fields in bad:
+        with pytest.raises(ValueError):
+            _lib.call("optx_sorted_create", ctypes.byref(_lib.CSortedConfig(*fields)), ctypes.byref(h))
+        assert not h.value
+    with pytest.raises(ValueError):
+        _lib.call("optx_sorted_create", None, None)
+    with pytest.raises(ValueError):
+        _lib.call("optx_sorted_run", None, None, None, None, 10, 0, None, None, None)
+    with pytest.raises(ValueError):
+        _lib.call("optx_sorted_stats", None, None, None)
+    assert lib.optx_sorted_destroy(None) == 0
 
 
 def test_no_silent_cpu_fallback_without_gpu(lib):
