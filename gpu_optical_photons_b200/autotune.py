@@ -25,6 +25,11 @@ cadence, chunk, tail steps and queue depth around the best point. Each candidate
 CUDA events on the launching stream (median of `repeats` runs after one warm-up
 run), on the real workload. Every candidate computes the same tallies (the
 engine's results do not depend on these settings), which `tune` checks.
+
+`tune_sorted` does the same for the per-interaction sorted kernels of one
+configuration: register budget (3 or 4 blocks of 256 threads per SM) x queue
+capacity (photons in flight), exhaustively; the best budget differs between
+workloads (the divergent Lambertian cube prefers 4, the long specular bar 3).
 """
 from __future__ import annotations
 
@@ -36,7 +41,7 @@ from dataclasses import asdict, replace
 import numpy as np
 
 from .params import TallyConfig
-from .wavefront import WaveConfig, WavefrontEngine
+from .wavefront import SortedEngine, WaveConfig, WavefrontEngine
 
 
 def time_config(cfg: WaveConfig, events, counts, tally: TallyConfig, repeats: int = 3,
@@ -128,6 +133,46 @@ def tune(events, counts, tally: TallyConfig, base: WaveConfig | None = None, rep
         if ms < best_ms:
             best_cfg, best_ms = cfg, ms
     return best_cfg, log
+
+
+def tune_sorted(p, tally: TallyConfig, n: int, budgets=(3, 4),
+                capacities=(1 << 20, 1 << 21, 1 << 22), repeats: int = 3, math="fast"):
+    """Best (blocks_per_sm, capacity) of the sorted kernels for n photons of the
+    configuration p, by CUDA-event timing (median of `repeats` after a warm-up
+    run). Returns (best, table) with table[(blocks_per_sm, capacity)] = ms;
+    raises if two candidates give different tallies."""
+    import torch
+    table, ref = {}, None
+    for bps, cap in itertools.product(budgets, capacities):
+        eng = SortedEngine(cap, 0, math, blocks_per_sm=bps)
+        try:
+            out = torch.zeros(tally.length, dtype=torch.int64, device="cuda")
+
+            def run():
+                out.zero_()
+                eng.run(p, n, tally=tally, tally_out=out)
+
+            run()
+            eng.stats()  # warm-up; raises on a failed run
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ms = []
+            for _ in range(repeats):
+                s.record()
+                run()
+                e.record()
+                torch.cuda.synchronize()
+                ms.append(s.elapsed_time(e))
+            eng.stats()
+        finally:
+            eng.close()
+        t = out.cpu().numpy()
+        if ref is None:
+            ref = t
+        elif not np.array_equal(t, ref):
+            raise RuntimeError(f"sorted run at blocks_per_sm={bps}, capacity={cap} changed the tally")
+        table[(bps, cap)] = float(np.median(ms))
+    best = min(table, key=table.get)
+    return {"blocks_per_sm": best[0], "capacity": best[1]}, table
 
 
 def main(argv=None):

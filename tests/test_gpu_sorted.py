@@ -196,3 +196,17 @@ def test_history_and_engine_wrappers_check_their_buffers(engine):
     eng.run_records(out)
     eng.close()
     assert compare_histories(records_to_numpy(out), records_to_numpy(records_device(p, 1000)))["bitwise_identical"] == 1000
+
+
+def test_sorted_autotuner_picks_a_measured_setting(engine):
+    from gpu_optical_photons_b200.autotune import tune_sorted
+    p, c = P.config2()
+    n = 2_000_000
+    best, table = tune_sorted(p, c, n, capacities=(1 << 16, 1 << 18), repeats=2)
+    assert set(table) == {(b, k) for b in (3, 4) for k in (1 << 16, 1 << 18)}
+    assert table[(best["blocks_per_sm"], best["capacity"])] == min(table.values())
+    eng = SortedEngine(best["capacity"], blocks_per_sm=best["blocks_per_sm"])
+    got, _ = eng.run(p, n, tally=c)
+    eng.stats()
+    eng.close()
+    assert np.array_equal(got.cpu().numpy(), tally_device(p, c, n).cpu().numpy())
