@@ -50,6 +50,12 @@ QUEUE_BYTES_PER_SPILL = 128
 SMS, FP32_LANES_PER_SM = 148, 128
 
 
+def workload_name(n_events: int) -> str:
+    """The benchmarked workload, named identically by both arms."""
+    return (f"batched events: {n_events} events, lognormal photons/event (median 1e4, sigma 1, "
+            "[1e2,1e6]), Lambertian cube, per-event tallies")
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -67,13 +73,19 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint replay / forward cost measurement")
     ap.add_argument("--no-single-configs", action="store_true",
-                    help="skip the single-configuration legs (configs 2 and 3 at 1e8 photons)")
+                    help="skip the single-configuration legs (four setups at their specified sizes)")
     ap.add_argument("--no-compaction", action="store_true",
                     help="skip the forced-compaction leg (state-queue HBM traffic)")
     ap.add_argument("--no-other-math", action="store_true",
                     help="skip timing the same batch in the other two math modes")
     ap.add_argument("--no-history-baseline", action="store_true",
                     help="skip the plain history-kernel baseline (one launch per event)")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the parity check of the benchmarked batch against the reference CPU run")
+    ap.add_argument("--no-ksweep", action="store_true",
+                    help="skip the history vs forced-compaction (k = 1, 4, 8) records leg")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip the reference's own GPU kernels (CPU value only)")
     ap.add_argument("--events", type=int, default=4096)
     ap.add_argument("--host-loop", action="store_true",
                     help="launch the waves from the host instead of the graph while loop "
@@ -161,13 +173,18 @@ def steps_of_tallies(t: np.ndarray) -> int:
     return int(t[:, -2].sum() + t[:, -1].sum() + t[:, 1].sum())
 
 
-def cpu_reference_leg(events, counts, tc, max_events: int, threads: int = 0, first: int = 0):
-    """Reference CPU tally (oracle/_ref) or the oracle port over events first .. max_events-1."""
+def cpu_reference_leg(events, counts, tc, max_events: int, threads: int = 0, first: int = 0,
+                      keep: bool = False):
+    """Reference CPU tally (oracle/_ref, the reference's default build) or the
+    oracle port over events first .. max_events-1, each event with its photon ids
+    offset_i .. offset_i + n_i - 1 (first_id = offset_i). Returns (cpu_baseline
+    dict, photon-steps/s, the per-event tallies when keep, else None)."""
     from oracle import oracle as O
     kind = "reference" if O.ref_available() else "port"
     offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
     steps = 0
     photons = 0
+    rows = []
     t0 = time.perf_counter()
     for i in range(first, max_events):
         if kind == "reference":
@@ -176,11 +193,88 @@ def cpu_reference_leg(events, counts, tc, max_events: int, threads: int = 0, fir
             t = O.tally(events[i], tc, int(counts[i]), int(offs[i]), threads=threads)
         steps += steps_of_tallies(t[None, :])
         photons += int(counts[i])
+        if keep:
+            rows.append(t)
     dt = time.perf_counter() - t0
     cores = (O.ref(0).ref_max_threads() if kind == "reference" else os.cpu_count()) if threads == 0 else threads
-    return {"value": steps / dt, "unit": UNIT, "cores": int(cores), "kind": kind,
-            "sample": f"events {first}..{max_events - 1} of {len(counts)} ({photons} photons, {steps} photon-steps), "
-                      f"run_cpu_tally per event, {dt:.1f} s"}, steps / dt
+    return ({"value": steps / dt, "unit": UNIT, "cores": int(cores), "kind": kind,
+             "sample": f"events {first}..{max_events - 1} of {len(counts)} ({photons} photons, {steps} photon-steps), "
+                       f"run_cpu_tally per event, {dt:.1f} s"}, steps / dt,
+            np.stack(rows) if keep else None)
+
+
+def chi2_two_sample(a, b):
+    """Two-sample chi-squared of two histograms with different totals (Numerical
+    Recipes 14.3, as the reference's include/optphot/stats.hpp): (chi2, ndf, p)."""
+    from scipy import stats as ss
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    A, B = a.sum(), b.sum()
+    m = (a + b) > 0
+    d = np.sqrt(B / A) * a[m] - np.sqrt(A / B) * b[m]
+    chi2 = float((d * d / (a[m] + b[m])).sum())
+    ndf = int(m.sum()) - 1
+    return chi2, ndf, float(ss.chi2.sf(chi2, ndf)) if ndf > 0 else 1.0
+
+
+def parity_leg(gpu_tallies, cpu_tallies, events, counts, tc, cfg, math: str, k_records: int = 64) -> dict:
+    """The benchmarked batch against the reference CPU run of the same photons.
+
+    Tallies (events 0 .. len(cpu_tallies) - 1): detected counts, per-event fate
+    counts (at least sum |delta| / 2 photons changed fate) and the two-sample
+    chi-squared p of the summed arrival-time histogram and hit map. Records
+    (events 0 .. k_records - 1): the same engine variant in batched records mode
+    against the reference CPU's records, photon by photon (fate and discrete
+    history agreement, the reference's compare_histories)."""
+    import torch
+    from oracle import oracle as O
+    from gpu_optical_photons_b200.backend import device_records, records_to_numpy
+    from gpu_optical_photons_b200.wavefront import WavefrontEngine
+    ne = len(cpu_tallies)
+    g = np.asarray(gpu_tallies[:ne], np.uint64)
+    c = np.asarray(cpu_tallies, np.uint64)
+    photons = int(c[:, :5].sum())
+    d_det = g[:, 0].astype(np.int64) - c[:, 0].astype(np.int64)
+    d_fates = int(np.abs(g[:, :5].astype(np.int64) - c[:, :5].astype(np.int64)).sum())
+    t0, x0 = 5, 5 + tc.time_bins + 1
+    _, _, p_time = chi2_two_sample(g[:, t0:x0].sum(axis=0), c[:, t0:x0].sum(axis=0))
+    _, _, p_hit = chi2_two_sample(g[:, x0:x0 + tc.xy_bins ** 2].sum(axis=0), c[:, x0:x0 + tc.xy_bins ** 2].sum(axis=0))
+    out = {"events": ne, "photons": photons, "gpu_math": math,
+           "cpu": "reference run_cpu_tally (default build)" if O.ref_available() else "oracle port (default math)",
+           "detected_gpu": int(g[:, 0].sum()), "detected_cpu": int(c[:, 0].sum()),
+           "abs_delta_detected_over_photons": int(np.abs(d_det).sum()) / photons,
+           "fate_count_changes_lower_bound_frac": d_fates / 2 / photons,
+           "chi2_p_time_hist": p_time, "chi2_p_hit_map": p_hit,
+           "total_photons_equal": int(g[:, :5].sum()) == photons}
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
+    k = min(k_records, len(events))
+    m = int(offs[k])
+    eng = WavefrontEngine(tc, k, m, cfg)
+    try:
+        eng.set_events(events[:k], counts[:k])
+        d = device_records(m)
+        eng.run_records(d)
+        torch.cuda.synchronize()
+        rec = records_to_numpy(d)
+        del d
+    finally:
+        eng.close()
+    same_fate = same_disc = 0
+    for i in range(k):
+        lo, hi = int(offs[i]), int(offs[i + 1])
+        if O.ref_available():
+            r, _ = O.ref_records(events[i], hi - lo, lo)
+        else:
+            r = O.records(events[i], hi - lo, lo)
+        f = rec["fate"][lo:hi] == r["fate"]
+        same_fate += int(f.sum())
+        same_disc += int((f & (rec["n_boundary"][lo:hi] == r["n_boundary"])
+                          & (rec["n_scatter"][lo:hi] == r["n_scatter"])).sum())
+    out["records"] = {"events": k, "photons": m, "fate_agreement": same_fate / m,
+                      "same_discrete_history": same_disc / m}
+    out["pass"] = bool(out["abs_delta_detected_over_photons"] <= 1e-3 and p_time > 0.01 and p_hit > 0.01
+                       and out["records"]["fate_agreement"] >= 0.999 and out["total_photons_equal"])
+    return out
 
 
 def history_baseline(g, events, counts, tc, first_id: int, math: str, stream, reps: int = 2):
@@ -246,7 +340,41 @@ def adjoint_cost(math: str, n: int = 10_000_000, reps: int = 5) -> dict:
             _lib.call("optx_engine_run_adjoint", m.engine._h, ctypes.c_void_p(wd.data_ptr()), 0.5,
                       ctypes.c_void_p(gd.data_ptr()), ctypes.c_void_p(st))
 
-        fwd, adj, fd = [], [], []
+        mom = torch.empty((tcal.time_bins + 1) * 5, dtype=torch.float64, device="cuda")
+
+        def moments_run():
+            _lib.call("optx_engine_run_score_moments", m.engine._h, ctypes.c_void_p(mom.data_ptr()),
+                      ctypes.c_void_p(st))
+
+        # The loss's gradient in one pass: the score-moment replay gives the
+        # histogram h and its Jacobian J = dE[h]/dtheta from the same photons, so
+        # the loss (Poisson NLL of h against a target, plus the detected
+        # fraction D = sum h / n) and its gradient J^T dL/dh + sum_b J_b / n come
+        # from one run; the host does the 500 x 4 product.
+        target = np.asarray(m.forward((800.0, 600.0, 0.93, 3.5))[0], np.float64)
+        m._upload(theta)
+        moments_run()
+        torch.cuda.synchronize()
+
+        def one_pass_gradient():
+            moments_run()
+            M = mom.view(tcal.time_bins + 1, 5).cpu().numpy()   # synchronises
+            h, J = M[:, 0], M[:, 1:]
+            lam = h[:tcal.time_bins] + 1.0
+            dl_dh = np.zeros_like(h)
+            dl_dh[:tcal.time_bins] = (1.0 - target[:tcal.time_bins] / lam) / n
+            dl_dh += 1.0 / n                                      # dD/dh_b
+            loss = float((lam - target[:tcal.time_bins] * np.log(lam)).sum() / n + h.sum() / n)
+            return loss, J.T @ dl_dh
+
+        def forward_loss():
+            m.engine.run_tally()
+            flat = m.engine.tallies()                            # synchronises
+            h = flat[0, 5:5 + tcal.time_bins + 1].astype(np.float64)
+            lam = h[:tcal.time_bins] + 1.0
+            return float((lam - target[:tcal.time_bins] * np.log(lam)).sum() / n + h.sum() / n)
+
+        fwd, adj, fd, one, one_wall, fwd_wall = [], [], [], [], [], []
         for _ in range(reps):
             m._upload(theta)  # back at theta after the FD runs (outside the timed regions)
             torch.cuda.synchronize()
@@ -264,11 +392,31 @@ def adjoint_cost(math: str, n: int = 10_000_000, reps: int = 5) -> dict:
                     m.engine.run_tally()
             b.record(); torch.cuda.synchronize()
             fd.append(a.elapsed_time(b))
+            m._upload(theta)
+            torch.cuda.synchronize()
+            a.record(); moments_run(); b.record(); torch.cuda.synchronize()
+            one.append(a.elapsed_time(b))
+            t0 = time.perf_counter(); one_pass_gradient(); one_wall.append((time.perf_counter() - t0) * 1e3)
+            t0 = time.perf_counter(); forward_loss(); fwd_wall.append((time.perf_counter() - t0) * 1e3)
+        # The one-pass gradient equals the replay of dL/dh (same photons).
+        loss, g1 = one_pass_gradient()
+        lam = np.asarray(m.forward(theta)[0])[:tcal.time_bins] + 1.0
+        wb = torch.zeros(tcal.time_bins + 1, dtype=torch.float64)
+        wb[:tcal.time_bins] = torch.from_numpy((1.0 - target[:tcal.time_bins] / lam) / n)
+        g2 = m.replay(theta, wb, 1.0 / n)
+        agree = float(np.max(np.abs(g1 - g2) / np.maximum(np.abs(g2), 1e-300)))
     finally:
         m.close()
     f, r, c = float(np.median(fwd)), float(np.median(adj)), float(np.median(fd))
+    o, ow, fw = float(np.median(one)), float(np.median(one_wall)), float(np.median(fwd_wall))
     return {"forward_ms": f, "replay_ms": r, "replay_over_forward": r / f,
             "crn_fd_ms": c, "adjoint_over_crn_fd": (f + r) / c, "photons": n,
+            "one_pass": {"moments_ms": o, "over_forward": o / f,
+                         "gradient_wall_ms": ow, "forward_loss_wall_ms": fw, "wall_over_forward": ow / fw,
+                         "max_rel_diff_vs_replay_gradient": agree,
+                         "what": "loss and its gradient from one score-moment replay (histogram + Jacobian, "
+                                 "J^T dL/dh on the host) against one forward run; wall times include the "
+                                 "read-back of the tally / moment table and the host arithmetic"},
             "what": "adjoint = one forward + one replay; CRN FD = 8 forward runs (2 per parameter)",
             "setup": "Lambertian cube, Rayleigh, volume source, theta=(1000, 700, 0.95, 4), 500 time bins"}
 
@@ -315,57 +463,84 @@ def run_reference(args):
     from gpu_optical_photons_b200.wavefront import batched_events
     events, counts = batched_events(n_events=args.events)
     tc = TallyConfig(100, 50.0, 10)
-    per_step = min(512, len(events))
-    vals = []
-    for s in range(args.warmup + args.steps):
-        lo = (s * per_step) % len(events)
-        base, v = cpu_reference_leg(events, counts, tc, lo + per_step, first=lo)
-        if s >= args.warmup:
-            vals.append(v)
+    # Warm-up steps run a 256-event slice (thread pool, page faults); every timed
+    # step runs the whole batch, the workload of the optx arm's value.
+    warm = min(256, len(events))
+    for s in range(args.warmup):
+        cpu_reference_leg(events, counts, tc, warm)
+    vals, secs = [], []
+    base = None
+    for s in range(args.steps):
+        t0 = time.perf_counter()
+        base, v, _ = cpu_reference_leg(events, counts, tc, len(events))
+        secs.append(time.perf_counter() - t0)
+        vals.append(v)
     value = float(np.median(vals))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"batched events ({args.events}), reference CPU run_cpu_tally",
-                       "per_step_sample": f"{per_step} events"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median(secs)) * 1e3,
+            "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded event generator)",
+            "config": {"workload": workload_name(len(events)),
+                       "events": len(events), "photons_per_step": int(counts.sum()),
+                       "per_step": "the whole batch: run_cpu_tally per event (all host threads)",
+                       "warmup_steps": f"{warm}-event slice"},
             "cpu_baseline": {**base, "value": value,
-                             "sample": f"{per_step} consecutive events per step; " + base["sample"]},
+                             "sample": "the whole batch per step; " + base["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    rg = reference_gpu_leg(events, counts, tc)
-    if rg is not None:
-        line["reference_gpu"] = rg
-    rs = reference_gpu_single_configs()
-    if rs is not None:
-        line["reference_gpu_single_configs"] = rs
+    if not args.no_reference_gpu:
+        rg = reference_gpu_leg(events, counts, tc)
+        if rg is not None:
+            line["reference_gpu"] = rg
+        rs = reference_gpu_single_configs()
+        if rs is not None:
+            line["reference_gpu_single_configs"] = rs
+        rk = reference_gpu_ksweep()
+        if rk is not None:
+            line["reference_gpu_ksweep"] = rk
     print(json.dumps(line), flush=True)
 
 
-def single_config_legs(math: str, n: int = 100_000_000, reps: int = 3) -> dict:
-    """One configuration at its specified size (the wrapped-Lambertian cube with
-    Rayleigh scattering and the all-specular long bar, 1e8 photons each, tally
-    mode): the wavefront engine (host-call settings: 7 blocks of 128 threads),
-    the per-interaction sorted kernels (photons queued in HBM by pending
+def single_setups():
+    """The single configurations at their specified sizes: (name, params, tally,
+    photons). The polished cube (1e6 photons), the wrapped-Lambertian cube with
+    Rayleigh scattering (1e8), the long bar with its black -z face (1e8; per-face
+    surfaces, which the reference cannot express) and the same bar with all side
+    and end faces specular (1e8; the reference-compatible variant)."""
+    from gpu_optical_photons_b200.params import config1, config2, config3
+    return [("polished_cube", *config1(), 1_000_000),
+            ("wrapped_lambertian_rayleigh", *config2(), 100_000_000),
+            ("long_bar_black_minus_z", *config3(True), 100_000_000),
+            ("long_bar_specular", *config3(False), 100_000_000)]
+
+
+def _ev_ms(fn, reps: int) -> float:
+    """Median CUDA-event time of fn on the current stream after one warm-up call."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(); fn(); b.record(); torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    return float(np.median(ts))
+
+
+def single_config_legs(math: str, reps: int = 3) -> dict:
+    """One configuration at its specified size (single_setups(), tally mode): the
+    wavefront engine (host-call settings: 7 blocks of 128 threads), the
+    per-interaction sorted kernels (photons queued in HBM by pending
     interaction, one launch per iteration) and this library's history kernel.
-    Median CUDA-event kernel times. (The
+    Median CUDA-event kernel times; the three tallies are checked equal. (The
     reference's own kernels on the same workloads are timed by the reference
     arm, `--impl reference`.)"""
     import torch
     from gpu_optical_photons_b200 import backend as B
-    from gpu_optical_photons_b200.params import config2, config3
     from gpu_optical_photons_b200.wavefront import SortedEngine, WaveConfig, WavefrontEngine
-
-    def ev_ms(fn):
-        fn()
-        torch.cuda.synchronize()
-        ts = []
-        for _ in range(reps):
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(); fn(); b.record(); torch.cuda.synchronize()
-            ts.append(a.elapsed_time(b))
-        return float(np.median(ts))
+    ev_ms = lambda fn: _ev_ms(fn, reps)  # noqa: E731
 
     out = {}
-    for name, (p, c) in (("wrapped_lambertian_rayleigh", config2()), ("long_bar_specular", config3(False))):
+    for name, p, c, n in single_setups():
         eng = WavefrontEngine(c, 1, n, WaveConfig(blocks_per_sm=7, math=math))
         try:
             eng.set_events([p], [n])
@@ -375,16 +550,68 @@ def single_config_legs(math: str, n: int = 100_000_000, reps: int = 3) -> dict:
             eng.close()
         steps = int(t[-2] + t[-1] + t[1])
         dev = torch.zeros(c.length, dtype=torch.int64, device="cuda")
-        hist = ev_ms(lambda: B.tally_device(p, c, n, out=dev, math=math))
+
+        def hist_run():
+            dev.zero_()
+            B.tally_device(p, c, n, out=dev, math=math)
+        hist = ev_ms(hist_run)
+        ht = dev.cpu().numpy().astype(np.uint64)
         srt = SortedEngine(math=math)
         try:
-            sorted_ms = ev_ms(lambda: srt.run(p, n, tally=c, tally_out=dev))
+            def sorted_run():
+                dev.zero_()
+                srt.run(p, n, tally=c, tally_out=dev)
+            sorted_ms = ev_ms(sorted_run)
             sst = srt.stats()
+            stt = dev.cpu().numpy().astype(np.uint64)
         finally:
             srt.close()
+        assert np.array_equal(ht, t) and np.array_equal(stt, t), f"{name}: tallies differ between kernels"
         out[name] = {"photons": n, "photon_steps": steps, "wavefront_ms": wave, "history_ms": hist,
                      "sorted_ms": sorted_ms, "sorted_iterations": sst["iterations"],
-                     "wavefront_photon_steps_per_s": steps / (wave * 1e-3)}
+                     "wavefront_photon_steps_per_s": steps / (wave * 1e-3),
+                     "history_photon_steps_per_s": steps / (hist * 1e-3),
+                     "wavefront_over_history": hist / wave, "tallies_equal": True}
+    return out
+
+
+def ksweep_leg(math: str, n: int = 10_000_000, reps: int = 3) -> dict:
+    """The wrapped-Lambertian cube with Rayleigh scattering (1e7 photons, records
+    mode) as the reference's event benchmark runs it (apps/optphot_event_bench.cpp:
+    130-143): the history kernel against the wavefront engine with a forced
+    compaction every k steps (k = 1, 4, 8: the reference event kernel's steps
+    per launch) and with none (one wave), records checked bit-identical across
+    all runs. Median CUDA-event kernel times (host read-back excluded). The
+    reference's own kernels on the same workload are the reference arm's
+    `reference_gpu_ksweep`."""
+    import torch
+    from gpu_optical_photons_b200 import backend as B
+    from gpu_optical_photons_b200.params import config2
+    from gpu_optical_photons_b200.wavefront import WaveConfig, WavefrontEngine
+    p, c = config2()
+    d = B.device_records(n)
+    hist = _ev_ms(lambda: B.records_device(p, n, out=d, math=math), reps)
+    torch.cuda.synchronize()
+    want = {k: v.clone() for k, v in d.items()}
+    steps = int((want["n_boundary"].long().sum() + want["n_scatter"].long().sum()
+                 + (want["fate"] == 1).long().sum()).item())
+    out = {"photons": n, "photon_steps": steps, "history_ms": hist, "wavefront": {}}
+    for k in (0, 1, 4, 8):
+        eng = WavefrontEngine(c, 1, n, WaveConfig(blocks_per_sm=7, math=math, cadence=k))
+        try:
+            eng.set_events([p], [n])
+            ms = _ev_ms(lambda: eng.run_records(d), reps)
+            st = eng.stats()
+        finally:
+            eng.close()
+        torch.cuda.synchronize()
+        same = all(torch.equal(d[f], want[f]) for f in d)
+        assert same, f"records differ at cadence {k}"
+        out["wavefront"]["one_wave" if k == 0 else f"k{k}"] = {
+            "ms": ms, "waves": int(st["launches"]), "spills": int(st["spills"]),
+            "photon_steps_per_s": steps / (ms * 1e-3), "records_bitwise_equal_history": True}
+    del d, want
+    torch.cuda.empty_cache()
     return out
 
 
@@ -421,10 +648,38 @@ def reference_gpu_leg(events, counts, tc):
                     "(host buffers, allocation per call), same 4096-event batch and tally binning"}
 
 
-def reference_gpu_single_configs(n: int = 100_000_000, reps: int = 3):
+def reference_gpu_single_configs(reps: int = 3):
     """The reference's tally kernel (rebuilt for sm_100a) on the single
-    configurations the optx arm's `single_configs` key times (1e8 photons each):
-    median kernel time reported by its run_gpu_tally. None without the library
+    configurations the optx arm's `single_configs` key times that the reference
+    can express (every one but the long bar's black -z face): median kernel time
+    reported by its run_gpu_tally. None without the library or a GPU."""
+    from oracle import oracle as O
+    try:
+        import torch
+        if not (O.refgpu_available() and torch.cuda.is_available()):
+            return None
+    except Exception:
+        return None
+    out = {}
+    for name, p, c, n in single_setups():
+        if p.faces_c() is not None:  # per-face surfaces: not expressible in the reference
+            continue
+        O.refgpu_tally(p, c, n)  # warm-up
+        runs = [O.refgpu_tally(p, c, n) for _ in range(reps)]
+        t = runs[0][0]
+        steps = steps_of_tallies(t[None, :])
+        kms = float(np.median([tm["kernel_ms"] for _, tm in runs]))
+        out[name] = {"photons": n, "photon_steps": steps, "kernel_ms": kms,
+                     "kernel_photon_steps_per_s": steps / (kms * 1e-3)}
+    return out
+
+
+def reference_gpu_ksweep(n: int = 10_000_000, reps: int = 3):
+    """The reference's records kernels (rebuilt for sm_100a) on the optx arm's
+    `ksweep` workload (wrapped-Lambertian cube, 1e7 photons): run_gpu_records
+    (history kernel) and run_gpu_records_event with k = 1, 4, 8 steps per launch
+    (compaction between launches); median kernel times as the reference reports
+    them (its event kernels' sum, host loop excluded). None without the library
     or a GPU."""
     from oracle import oracle as O
     try:
@@ -433,16 +688,21 @@ def reference_gpu_single_configs(n: int = 100_000_000, reps: int = 3):
             return None
     except Exception:
         return None
-    from gpu_optical_photons_b200.params import config2, config3
-    out = {}
-    for name, (p, c) in (("wrapped_lambertian_rayleigh", config2()), ("long_bar_specular", config3(False))):
-        O.refgpu_tally(p, c, n)  # warm-up
-        runs = [O.refgpu_tally(p, c, n) for _ in range(reps)]
-        t = runs[0][0]
-        steps = steps_of_tallies(t[None, :])
-        kms = float(np.median([tm["kernel_ms"] for _, tm in runs]))
-        out[name] = {"photons": n, "photon_steps": steps, "kernel_ms": kms,
-                     "kernel_photon_steps_per_s": steps / (kms * 1e-3)}
+    from gpu_optical_photons_b200.params import config2
+    p, _ = config2()
+    O.refgpu_records(p, n)  # warm-up
+    runs = [O.refgpu_records(p, n) for _ in range(reps)]
+    r0 = runs[0][0]
+    steps = int(r0["n_boundary"].astype(np.int64).sum() + r0["n_scatter"].astype(np.int64).sum()
+                + (r0["fate"] == 1).sum())
+    out = {"photons": n, "photon_steps": steps,
+           "history_kernel_ms": float(np.median([tm["kernel_ms"] for _, tm in runs])), "event": {}}
+    for k in (1, 4, 8):
+        O.refgpu_records_event(p, n, k)  # warm-up
+        ev = [O.refgpu_records_event(p, n, k) for _ in range(reps)]
+        out["event"][f"k{k}"] = {"kernels_ms": float(np.median([st["kernels_ms"] for _, st, _ in ev])),
+                                 "total_ms": float(np.median([tm["total_ms"] for _, _, tm in ev])),
+                                 "launches": ev[0][1]["launches"]}
     return out
 
 
@@ -545,13 +805,17 @@ def run_optx(args):
     peak_mhz = clocks["sm_max_mhz"] or 1965.0
     peak_gops = SMS * FP32_LANES_PER_SM * peak_mhz * 1e6 / 1e9
     achieved_gops = OPS_PER_STEP * steps_per_run / (ms_step * 1e-3) / 1e9
+    # DRAM bytes (read + write) of the wave kernel over one run of this batch,
+    # from an ncu capture of the benchmarked batch itself (profiles/); the
+    # tallies, event records and queues it moves scale with events, not steps,
+    # so only a capture of the same batch gives the per-step figure.
     traffic = None
     prof = os.path.join(HERE, "profiles", "wave_kernel_batched.json")
     if os.path.exists(prof):
         with open(prof) as f:
-            bps = json.load(f).get("dram_bytes_per_photon_step")
-        if bps:
-            traffic = bps * steps_per_run
+            pj = json.load(f)
+        if pj.get("events") == len(events) and pj.get("photons") == n_photons:
+            traffic = pj.get("dram_bytes_per_run")
     queue_bytes = QUEUE_BYTES_PER_SPILL * int(st["spills"])
     peaks = {}
     peaks_path = os.path.join(HERE, "MEASURED_PEAKS.json")
@@ -564,8 +828,7 @@ def run_optx(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded event generator)",
-        "config": {"workload": "batched events: 4096 events, lognormal photons/event (median 1e4, "
-                               "sigma 1, [1e2,1e6]), Lambertian cube, per-event tallies",
+        "config": {"workload": workload_name(len(events)),
                    "events": len(events), "photons_per_step": n_photons,
                    "photon_steps_per_step": steps_per_run, "photons_per_s": world * n_photons / (ms_step * 1e-3),
                    "l2": "flushed between timed steps (256 MB write, outside the CUDA events)",
@@ -642,9 +905,18 @@ def run_optx(args):
             "what": "one history-kernel launch (optx_tally_device) per event, back to back on one "
                     "stream; identical tallies checked",
             "speedup_of_value": value / (world * hv)}
+    if not args.no_ksweep:
+        line["ksweep"] = ksweep_leg(args.math)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:  # the CPU baseline is an N=1 figure
-        base, _ = cpu_reference_leg(events, counts, tc, max_events=min(1024, len(events)))
+        # All host threads on events 0..1023, then one thread on events 0..255
+        # (the reference's threads = n and threads = 1, apps/optphot_bench.cpp:125-158).
+        base, _, cpu_t = cpu_reference_leg(events, counts, tc, max_events=min(1024, len(events)),
+                                           keep=not args.no_parity and first_id == 0)
+        one, _, _ = cpu_reference_leg(events, counts, tc, max_events=min(256, len(events)), threads=1)
+        base["single_thread"] = one
         line["cpu_baseline"] = base
+        if cpu_t is not None:
+            line["parity"] = parity_leg(tallies, cpu_t, events, counts, tc, cfg, args.math)
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

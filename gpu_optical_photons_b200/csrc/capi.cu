@@ -177,6 +177,10 @@ int ensure_device() {
   return OPTX_OK;
 }
 
+// Forgets the looked-up device addresses of the allocation-free call's static
+// scratch (defined with that call, at the end of this file).
+void noalloc_forget_addresses();
+
 int num_sms() {
   int dev = 0, n = 0;
   cudaGetDevice(&dev);
@@ -966,6 +970,9 @@ int optx_release_cache(void) {
     if (g_cache.e1) cudaEventDestroy(g_cache.e1);
     g_cache = Cache{};
     engines.swap(g_api);
+    // After a device reset the module is loaded again, possibly elsewhere: the
+    // next allocation-free call looks the scratch address up afresh.
+    noalloc_forget_addresses();
   }
   engines.clear();  // an engine still used by a call is destroyed when that call ends
   return OPTX_OK;
@@ -1974,6 +1981,9 @@ int optx_sorted_run(optx_sorted* s, const optx_params* p, const optx_faces* face
   const unsigned long long bound =
       (n / s->cap + 2ull) * (static_cast<unsigned long long>(P.max_steps) + 2ull) + 64ull;
   a.iter_cap = test_fault("watchdog") ? 1u : static_cast<uint32_t>(std::min(bound, 0xfffffff0ull));
+  // One set of queues and one control block per handle: a run on another stream
+  // waits on the device for the previous run to end.
+  if (s->ran) OPTX_CUDA(cudaStreamWaitEvent(st, s->ev1, 0));
   OPTX_CUDA(cudaEventRecord(s->ev0, st));
   s->ran = true;
   if (!s->host_loop) {
@@ -2046,6 +2056,12 @@ void* g_noalloc_ptr[kNoAllocMaxDevices] = {};  // device address of the array, p
 
 }  // namespace
 
+namespace {
+void noalloc_forget_addresses() {  // called with g_mu held, like the allocation-free call
+  for (void*& p : g_noalloc_ptr) p = nullptr;
+}
+}  // namespace
+
 extern "C" int optx_wavefront_tally_noalloc(const optx_params* p, const optx_faces* faces,
                                             const optx_tally_config* c, uint64_t n,
                                             uint64_t first_id, uint64_t* tally_out, int math,
@@ -2055,11 +2071,6 @@ extern "C" int optx_wavefront_tally_noalloc(const optx_params* p, const optx_fac
   OPTX_TRY(check_math(math));
   TallyDev td{};
   OPTX_TRY(make_tally_dev(c, td));
-  if (td.len > kNoAllocMaxTally)
-    return fail(OPTX_ERR_INVALID_ARGUMENT,
-                "optx_wavefront_tally_noalloc: tally length " + std::to_string(td.len) +
-                    " exceeds the static scratch maximum of " + std::to_string(kNoAllocMaxTally) +
-                    " entries (5 + time_bins + 1 + xy_bins^2 + 2)");
   if (n > 0xffffffffull)
     return fail(OPTX_ERR_INVALID_ARGUMENT,
                 "optx_wavefront_tally_noalloc: at most 2^32 - 1 photons per call");
@@ -2072,6 +2083,23 @@ extern "C" int optx_wavefront_tally_noalloc(const optx_params* p, const optx_fac
   int dev = 0;
   OPTX_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(OPTX_ERR_RUNTIME, "device ordinal out of range");
+  constexpr int kBlock = 256, kMinB = 4;
+  // The histograms sit in shared memory beside the 8 warps' pantries, so the
+  // longest tally is what the opt-in shared memory per block leaves (B200:
+  // 232,448 B), capped by the static tally accumulator.
+  int max_optin = 0;
+  OPTX_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa{};
+  OPTX_CUDA(cudaFuncGetAttributes(&fa, DISPATCH(math, wave_kernel_fn, kModeTally, kSingle, kMinB)));
+  const long long pantries = static_cast<long long>(kBlock / 32) * kPantryBytesPerWarp;
+  const long long room = static_cast<long long>(max_optin) - static_cast<long long>(fa.sharedSizeBytes) - pantries;
+  const uint64_t max_len = std::min<uint64_t>(kNoAllocMaxTally, room > 0 ? static_cast<uint64_t>(room / 4) + 7u : 0u);
+  if (td.len > max_len)
+    return fail(OPTX_ERR_INVALID_ARGUMENT,
+                "optx_wavefront_tally_noalloc: tally length " + std::to_string(td.len) +
+                    " exceeds the maximum of " + std::to_string(max_len) +
+                    " entries on this device (5 + time_bins + 1 + xy_bins^2 + 2; the histograms "
+                    "share the opt-in shared memory per block with the pantries)");
   // First call on this device: the host-side name of the array is not a device
   // address, so look the address up once (with this device current).
   if (g_noalloc_ptr[dev] == nullptr) {
@@ -2086,11 +2114,10 @@ extern "C" int optx_wavefront_tally_noalloc(const optx_params* p, const optx_fac
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
   const DevParams P = make_dev_params(*p, faces);
-  constexpr int kBlock = 256, kMinB = 4;
   const size_t smem = static_cast<size_t>(kBlock / 32) * kPantryBytesPerWarp +
                       static_cast<size_t>(td.len - 7u) * 4u;
-  if (smem > 48 * 1024) OPTX_CUDA(DISPATCH(math, wave_set_smem, kModeTally, false, kMinB, smem));
-  const int bps = DISPATCH(math, wave_blocks_per_sm, kModeTally, false, kMinB, kBlock, smem);
+  if (smem > 48 * 1024) OPTX_CUDA(DISPATCH(math, wave_set_smem, kModeTally, kSingle, kMinB, smem));
+  const int bps = DISPATCH(math, wave_blocks_per_sm, kModeTally, kSingle, kMinB, kBlock, smem);
   if (bps <= 0)
     return fail(OPTX_ERR_RUNTIME, "tally histograms need too much shared memory; reduce xy_bins / time_bins");
   const int grid = std::min(bps, kMinB) * num_sms();
@@ -2121,7 +2148,7 @@ extern "C" int optx_wavefront_tally_noalloc(const optx_params* p, const optx_fac
   // tally accumulator (the array keeps the previous call's contents).
   OPTX_CUDA(DISPATCH(math, launch_wave_prep, d_args, d_ctrl, std::min(grid, 4 * num_sms()), 256, st));
   for (;;) {
-    OPTX_CUDA(DISPATCH(math, launch_wave, kModeTally, false, kMinB, P, d_args, d_ctrl, grid, kBlock,
+    OPTX_CUDA(DISPATCH(math, launch_wave, kModeTally, kSingle, kMinB, P, d_args, d_ctrl, grid, kBlock,
                        smem, st));
     unsigned active = 0;
     OPTX_CUDA(cudaMemcpyAsync(&active, &d_ctrl->active, sizeof(active), cudaMemcpyDeviceToHost, st));

@@ -1,7 +1,7 @@
 """Parameter and result structures of the optx C ABI (include/optx.h).
 
 ``SimParams`` has the byte layout of the reference's ``optphot::SimParams``
-(include/optphot/params.hpp:86-109, 72 bytes) so that the same 72 bytes can be
+(include/optphot/params.hpp:40-63, 72 bytes) so that the same 72 bytes can be
 handed to the reference backend, to this engine's C ABI and to the oracle.
 ``TallyConfig`` mirrors include/optphot/transport.hpp:164-168 and the enums
 mirror include/optphot/params.hpp:61-84.
@@ -58,7 +58,7 @@ class CTallyConfig(ctypes.Structure):
 
 @dataclass
 class SimParams:
-    """Python view of one simulation setup; defaults are the reference's (params.hpp:86-109)."""
+    """Python view of one simulation setup; defaults are the reference's (params.hpp:40-63)."""
 
     hx: float = 25.0
     hy: float = 25.0

@@ -224,11 +224,15 @@ class SortedEngine:
             pass
 
     def run(self, p: SimParams, n: int, first_id: int = 0, tally: TallyConfig | None = None,
-            tally_out=None, records_out=None, stream=None):
+            tally_out=None, records_out=None, stream=None, check: bool = False):
         """Runs n photons. With `tally` set, ADDS into `tally_out` (a torch int64
         device tensor of tally.length; a zeroed one is made when None). Records
         go into `records_out` (a dict from backend.device_records) when given.
-        Returns (tally_out, records_out)."""
+        Returns (tally_out, records_out).
+
+        The run is asynchronous: a queue overflow or a watchdog stop is reported
+        only by the next `stats()` call. With check=True the call synchronises
+        the stream and raises on those errors (as `stats()` does)."""
         import torch
         if tally is not None and tally_out is None:
             tally_out = torch.zeros(tally.length, dtype=torch.int64, device="cuda")
@@ -244,6 +248,8 @@ class SortedEngine:
                   ctypes.byref(cc) if cc is not None else None, n, first_id,
                   ctypes.c_void_p(tally_out.data_ptr()) if tally is not None else None,
                   ctypes.byref(cr) if cr is not None else None, _stream_ptr(stream))
+        if check:
+            self.stats(stream)
         return tally_out, records_out
 
     def stats(self, stream=None) -> dict:

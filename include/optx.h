@@ -42,7 +42,7 @@ extern "C" {
 #define OPTX_MATH_EXACT 1
 #define OPTX_MATH_APPROX 2
 
-/* optphot::SimParams, byte for byte (include/optphot/params.hpp:86-109). */
+/* optphot::SimParams, byte for byte (include/optphot/params.hpp:40-63). */
 typedef struct optx_params {
   float hx, hy, hz;
   float n_scint, n_det, n_out, abs_length, scat_length;
@@ -216,7 +216,9 @@ int optx_sorted_destroy(optx_sorted* s);
 /* n photons (ids first_id ..) of one configuration, async on `stream`: ADDS the
  * tally into dev_tally (flat layout as optx_run_tally; NULL = none) and writes
  * dev_records (n entries; NULL = none). n < 2^32. Run errors are reported by
- * the next optx_sorted_stats. */
+ * the next optx_sorted_stats. A handle has one set of queues: a run given a
+ * different stream than the previous run waits on the device for that run to
+ * end (runs of one handle never overlap). */
 int optx_sorted_run(optx_sorted* s, const optx_params* p, const optx_faces* faces,
                     const optx_tally_config* c, uint64_t n, uint64_t first_id,
                     uint64_t* dev_tally, const optx_records* dev_records, void* stream);
@@ -325,10 +327,15 @@ int optx_run_gensteps(optx_engine* e, const optx_params* events, const optx_face
  * optx_run_tally (the wavefront engine on one configuration, host output), with
  * all device scratch in a static 2.6 MiB array of the library that every GPU
  * loading liboptx.so holds until the process exits. It calls no cudaMalloc,
- * cudaFree or other allocating routine. Limits: tally length (5 + time_bins + 1 +
- * xy_bins^2 + 2) <= 65536 entries and n < 2^32; larger requests fail with
- * OPTX_ERR_INVALID_ARGUMENT. The first call on a device looks up the array's
- * device address (make that first call before any stream capture). Every call
+ * cudaFree or other allocating routine. Limits: n < 2^32, and a tally length
+ * (5 + time_bins + 1 + xy_bins^2 + 2) of at most (the device's opt-in shared
+ * memory per block - the kernel's static shared memory - 28,672 B of photon
+ * pantries) / 4 + 7 entries, capped at 65,536 by the array: 50,927 entries on
+ * B200. Larger requests fail with OPTX_ERR_INVALID_ARGUMENT before any launch,
+ * and the message gives the device's maximum. The first call on a device looks
+ * up the array's device address (make that first call before any stream
+ * capture; optx_release_cache makes the next call look it up again, e.g. after
+ * a cudaDeviceReset). Every call
  * shares the one array: calls that overlap on the GPU (other streams or host
  * threads) race; the library serialises calls from one process. Synchronous on
  * `stream`; tally_out is a host array, overwritten. */

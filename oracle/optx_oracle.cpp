@@ -17,7 +17,7 @@
 //   src/cpu/cpu_backend.cpp        records / tally loops
 // with the same floating-point expression order, so that, compiled with
 // -ffp-contract=off, it reproduces the reference CPU build bit for bit (pinned
-// by tests/test_oracle_pin.py against the reference compiled from its own
+// by tests/test_oracle_golden.py against the reference compiled from its own
 // sources, and by the golden fixtures in tests/golden/).
 //
 // Extensions beyond the reference (each keeps the reference draw order):
@@ -39,7 +39,7 @@
 namespace oracle {
 
 // ---------------------------------------------------------------------------
-// Parameters: byte layout of SimParams (include/optphot/params.hpp:86-109).
+// Parameters: byte layout of SimParams (include/optphot/params.hpp:40-63).
 struct Params {
   float hx, hy, hz;
   float n_scint, n_det, n_out, abs_length, scat_length;

@@ -28,13 +28,26 @@ _P = ctypes.c_void_p
 _u64 = ctypes.c_uint64
 
 
+def reference_root() -> str:
+    """The reference checkout: the OPTX_REFERENCE environment variable, else the
+    default of the build recipe (oracle/Makefile's REF), asked from make."""
+    env = os.environ.get("OPTX_REFERENCE")
+    if env:
+        return env
+    r = subprocess.run(["make", "-s", "--no-print-directory", "-C", HERE, "print-ref"],
+                       capture_output=True, text=True, check=False)
+    return r.stdout.strip() if r.returncode == 0 else ""
+
+
 def build(with_ref: bool = True) -> None:
     """Builds the oracle (and the reference backend when its checkout is present)."""
     targets = ["all"]
-    if with_ref and os.path.isdir(os.environ.get("OPTX_REFERENCE", "/root/reference")):
+    ref_dir = reference_root()
+    if with_ref and ref_dir and os.path.isdir(ref_dir):
         targets.append("ref")
     env = dict(os.environ)
-    env.setdefault("REF", os.environ.get("OPTX_REFERENCE", "/root/reference"))
+    if ref_dir:
+        env["REF"] = ref_dir
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True, env=env)
 
 

@@ -25,6 +25,8 @@ libref_gpu_portable.so, to compare this repository's kernels with the
 reference kernels on the same B200.
 
     python oracle/relink.py [--ref DIR] [--force]
+
+The reference checkout defaults to OPTX_REFERENCE, else to oracle/Makefile's REF.
 """
 from __future__ import annotations
 
@@ -37,6 +39,9 @@ from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+from oracle.oracle import reference_root  # noqa: E402  (the checkout: OPTX_REFERENCE or the Makefile's REF)
 OUT = os.path.join(HERE, "_ref", "relink")
 LIBDIR = os.path.join(ROOT, "gpu_optical_photons_b200")
 SHIM = os.path.join(LIBDIR, "shim", "optx_backend.cpp")
@@ -92,8 +97,9 @@ GPU_FLAVOURS = {
 }
 
 
-def build_ref_gpu(ref: str = "/root/reference", force: bool = False) -> list[str]:
+def build_ref_gpu(ref: str | None = None, force: bool = False) -> list[str]:
     """The reference's GPU backend for sm_100a, one shared library per flavour."""
+    ref = ref or reference_root()
     if not os.path.isdir(os.path.join(ref, "src", "gpu")):
         return []
     out_dir = os.path.join(HERE, "_ref")
@@ -115,9 +121,10 @@ def build_ref_gpu(ref: str = "/root/reference", force: bool = False) -> list[str
     return [os.path.join(out_dir, n) for n in GPU_FLAVOURS]
 
 
-def build(ref: str = "/root/reference", force: bool = False) -> str | None:
+def build(ref: str | None = None, force: bool = False) -> str | None:
     """Builds every program of both flavours; returns the output directory, or
     None when the reference checkout or liboptx.so is missing."""
+    ref = ref or reference_root()
     lib = os.path.join(LIBDIR, "liboptx.so")
     if not os.path.isdir(os.path.join(ref, "include", "optphot")) or not os.path.exists(lib):
         return None
@@ -151,7 +158,7 @@ def build(ref: str = "/root/reference", force: bool = False) -> str | None:
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference checkout (default: OPTX_REFERENCE, else the oracle Makefile's REF)")
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args(argv)
     build_ref_gpu(a.ref, a.force)

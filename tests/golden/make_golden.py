@@ -27,7 +27,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from gpu_optical_photons_b200 import params as P  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-REFERENCE = os.environ.get("OPTX_REFERENCE", "/root/reference")
+REFERENCE = O.reference_root()
 
 CASES = {
     # name: (SimParams, n, first_id)
