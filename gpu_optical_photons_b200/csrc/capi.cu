@@ -541,6 +541,7 @@ int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphC
   a.use_graph = (e->cfg.use_graph >= 0) ? 1u : 0u;
   a.chunk = e->cfg.chunk;
   a.tail_steps = e->cfg.tail_steps;
+  a.slot_cache = max_steps < kSlotMaxAdd ? 1u : 0u;  // bounds the u32 slot sums
   (void)grid;
   (void)batch;
   OPTX_CUDA(cudaMemcpyAsync(e->d_args, &a, sizeof(a), cudaMemcpyHostToDevice, st));

@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
   const uint32_t lt = (1u << lane) - 1u;
   const uint32_t nwarps = blockDim.x >> 5;
   // [pantries: nwarps x 32 x 112 B][block histograms (tally), bin weights (adjoint)
-  //  or, batched tally, per-warp event slots: nwarps x 2 x 8 u64 counters, then
+  //  or, batched tally, per-warp event slots: nwarps x 2 x 8 u32 counters, then
   //  nwarps x 2 x n_bins u32 bins when n_bins <= kSlotBins]
   constexpr bool kSlots = BATCH && MODE == kModeTally;
   constexpr bool kAdj = MODE == kModeAdjoint || MODE == kModeMoments;  // replay modes
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
   uint32_t* s_hist = reinterpret_cast<uint32_t*>(extra);
   double* s_w = reinterpret_cast<double*>(extra);
   double* s_mom = s_w + (A->tc.time_bins + 1u);  // adjoint, moments_smem: [time_bins + 1][5]
-  unsigned long long* s_evc = reinterpret_cast<unsigned long long*>(extra) + warp * 16u;
+  uint32_t* s_evc = reinterpret_cast<uint32_t*>(extra) + warp * 16u;
   __shared__ double s_red[4][16];
 
   // Wave-constant values live in shared memory, not in each thread's registers.
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     const float4* qin;
     float4* qout;
     unsigned long long fresh_next, first_id, iter_cap;
-    uint32_t n_in, items, T, cadence, qcap, chunk, ev_shift, tail_steps;
+    uint32_t n_in, items, T, cadence, qcap, chunk, ev_shift, tail_steps, slot_cache;
     const uint32_t* tally_of;
     TallyDev tc;
   };
@@ -285,6 +285,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     ws.tally_of = A->tally_of;
     ws.ev_shift = A->ev_shift;
     ws.tail_steps = A->tail_steps < 1u ? 1u : A->tail_steps;
+    ws.slot_cache = A->slot_cache;
     ws.tc = A->tc;
   }
   __syncthreads();
@@ -313,7 +314,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     for (uint32_t b = threadIdx.x; b < n_bins; b += blockDim.x) s_hist[b] = 0u;
   }
   if (kSlots) {
-    if (lane < 16u) s_evc[lane] = 0ull;
+    if (lane < 16u) s_evc[lane] = 0u;
     if (slot_bins) {
       for (uint32_t b = lane; b < 2u * n_bins; b += 32u) s_sb[b] = 0u;
     }
@@ -335,13 +336,26 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
   bool exhausted = false;  // warp-uniform: the wave's work items are all handed out
   uint32_t pc = 0u;        // warp-uniform: photons waiting in this warp's pantry
   uint32_t wsteps = 0u;
-  // Work items [chunk_lo, chunk_hi) claimed by this warp and not yet emitted (warp-uniform).
-  uint32_t chunk_lo = 0u, chunk_hi = 0u;
+  // Warp-uniform bookkeeping: the work items [chunk_lo, chunk_hi) claimed by this
+  // warp and not yet emitted; batched, the events cached in its two shared-memory
+  // slots and the slot replaced next. Batched variants keep these in shared
+  // memory (measured: fewer local-memory spills, -5 % per photon-step on the
+  // batch), the single-configuration ones in registers.
+  constexpr uint32_t kNoEvent = 0xffffffffu;
+  // [warp][chunk_lo, chunk_hi, tag0, tag1, victim, photons since the last slot flush]
+  __shared__ uint32_t s_book[8][8];
+  uint32_t r_book[6] = {0u, 0u, kNoEvent, kNoEvent, 0u, 0u};
+  uint32_t* book = BATCH ? s_book[warp] : r_book;
+  if (BATCH && lane < 6u) s_book[warp][lane] = (lane == 2u || lane == 3u) ? kNoEvent : 0u;
+  __syncwarp();
+  uint32_t& chunk_lo = book[0];
+  uint32_t& chunk_hi = book[1];
+  uint32_t& tag0 = book[2];
+  uint32_t& tag1 = book[3];
+  uint32_t& victim = book[4];
+  uint32_t& since = book[5];
   // Single configuration: per-lane tallies, flushed at the end of the wave.
   uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0, snb = 0, sns = 0;
-  // Batched: the events cached in this warp's two shared-memory slots (warp-uniform).
-  constexpr uint32_t kNoEvent = 0xffffffffu;
-  uint32_t tag0 = kNoEvent, tag1 = kNoEvent, victim = 0u;
   double g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
   uint32_t useful = 0u, iters = 0u;
 
@@ -352,10 +366,10 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     if (tag != kNoEvent) {
       unsigned long long* G = A->tally + static_cast<size_t>(tag) * tc.len;
       if (lane < 7u) {  // 5 fates, then the nb and ns sums (the last two entries)
-        const unsigned long long c = s_evc[v * 8u + lane];
-        if (c != 0ull) {
-          atomicAdd(&G[lane < 5u ? lane : tc.len - 7u + lane], c);
-          s_evc[v * 8u + lane] = 0ull;
+        const uint32_t c = s_evc[v * 8u + lane];
+        if (c != 0u) {
+          atomicAdd(&G[lane < 5u ? lane : tc.len - 7u + lane], static_cast<unsigned long long>(c));
+          s_evc[v * 8u + lane] = 0u;
         }
       }
       if (slot_bins) {
@@ -377,15 +391,19 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     if (MODE == kModeRecords) {
       store_record(A->rec, pidx, s, fate);
     } else if (MODE == kModeTally && BATCH) {
-      // Shared-memory atomics into the event's slot when the warp caches it,
-      // else global atomics into the event's slice.
+      // 32-bit shared-memory atomics into the event's slot when the warp caches
+      // it (a 64-bit shared add costs a compare-and-swap loop: measured -10 % per
+      // photon-step on the batch), else 64-bit global atomics into the event's
+      // slice. Events are cached only when every record's max_steps is below
+      // kSlotMaxAdd (so is each photon's nb and ns), and the warp flushes its
+      // slots every kSlotFlushPhotons photons (at a refill): no u32 counter wraps.
       const int slot = ev == tag0 ? 0 : (ev == tag1 ? 1 : -1);
       unsigned long long* G = A->tally + static_cast<size_t>(ev) * tc.len;
       if (slot >= 0) {
-        unsigned long long* C = s_evc + slot * 8;
-        atomicAdd(&C[fate], 1ull);
-        if (s.nb) atomicAdd(&C[5], static_cast<unsigned long long>(s.nb));
-        if (s.ns) atomicAdd(&C[6], static_cast<unsigned long long>(s.ns));
+        uint32_t* C = s_evc + slot * 8;
+        atomicAdd(&C[fate], 1u);
+        if (s.nb) atomicAdd(&C[5], s.nb);
+        if (s.ns) atomicAdd(&C[6], s.ns);
       } else {
         atomicAdd(&G[fate], 1ull);
         if (s.nb) atomicAdd(&G[tc.len - 2u], static_cast<unsigned long long>(s.nb));
@@ -478,8 +496,8 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     return done;
   };
 
-  for (unsigned long long it = 0;; ++it) {
-    if (it > iter_cap) {
+  for (;;) {
+    if (static_cast<unsigned long long>(iters) > iter_cap) {
       if (lane == 0u) atomicOr(&ctrl->error, kErrWatchdog);
       break;
     }
@@ -559,17 +577,35 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
           }
         }
         pc += got;
-        if (kSlots && got > 0u) {
-          // Cache the newest event in a slot; keep the slot of the oldest event
-          // of this refill if it has one, else replace the slots in turn.
-          const uint32_t e_first = __shfl_sync(kFull, nev, 0);
-          const uint32_t e_last = __shfl_sync(kFull, nev, got - 1u);
-          if (e_last != tag0 && e_last != tag1) {
-            const uint32_t v = tag0 == e_first ? 1u : (tag1 == e_first ? 0u : victim);
-            victim = v ^ 1u;
-            flush_slot(v, v == 0u ? tag0 : tag1);
-            if (v == 0u) tag0 = e_last; else tag1 = e_last;
+        if (kSlots) {
+          // Slots to flush (bit v: slot v), through one flush site. (1) u32 slot
+          // counters stay bounded: only photons that entered this warp through
+          // its pantry finish here, so flushing both slots once kSlotFlushPhotons
+          // photons have entered since the last flush keeps every counter below
+          // (kSlotFlushPhotons + 64) x kSlotMaxAdd < 2^32. (2) The newest event
+          // takes a slot: the slot of the oldest event of this refill is kept if
+          // it has one, else the slots are replaced in turn.
+          uint32_t fm = 0u, v = 2u, e_last = kNoEvent;
+          since += got;
+          if (since >= kSlotFlushPhotons) {
+            fm = 3u;
+            since = 0u;
           }
+          if (got > 0u && ws.slot_cache) {
+            const uint32_t e_first = __shfl_sync(kFull, nev, 0);
+            e_last = __shfl_sync(kFull, nev, got - 1u);
+            if (e_last != tag0 && e_last != tag1) {
+              v = tag0 == e_first ? 1u : (tag1 == e_first ? 0u : victim);
+              victim = v ^ 1u;
+              fm |= 1u << v;
+            }
+          }
+#pragma unroll 1
+          for (uint32_t j = 0; j < 2u; ++j) {
+            if (fm & (1u << j)) flush_slot(j, j == 0u ? tag0 : tag1);
+          }
+          if (v == 0u) tag0 = e_last;
+          if (v == 1u) tag1 = e_last;
         }
         __syncwarp();
       }
@@ -635,7 +671,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
     if (alive) {
       const DevParams& P = params_of<BATCH, UNI>(P0, A, ev);
       const bool still =
-          step_photon<kAdj>(P, s, r, first_id + pidx, fate, aux, smask);
+          step_photon<kAdj, BATCH && !UNI>(P, s, r, first_id + pidx, fate, aux, smask);
       ++wsteps;
       ended = !still || s.nb + s.ns >= P.max_steps;  // at max_steps fate stays kMaxSteps
     }

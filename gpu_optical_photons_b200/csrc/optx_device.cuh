@@ -213,7 +213,12 @@ struct ScoreAux {
   float t_emit;     // sampled emission time
 };
 
+// GP: P is a record in global memory, where an indexed load costs one
+// instruction; a kernel parameter is read with selects instead (indexing it
+// would copy the parameters to local memory).
+template <bool GP>
 __device__ __forceinline__ float face_refl(const DevParams& P, int face) {
+  if (GP) return (&P.refl0)[face];
   float r = P.refl0;
   r = (face == 1) ? P.refl1 : r;
   r = (face == 2) ? P.refl2 : r;
@@ -390,7 +395,7 @@ __device__ __forceinline__ uint32_t face_model(const DevParams& P, int face) {
 // step together) the warp reconverges before the advance, so the Philox block
 // runs once per warp step for all lanes that need one rather than once per
 // divergent group.
-template <bool AUX>
+template <bool AUX, bool GP = false>
 __device__ __forceinline__ bool step_act(const DevParams& P, Photon& s, Rng& r, uint64_t id,
                                          uint32_t& fate, ScoreAux& aux, int hit,
                                          uint32_t sync_mask = 0u) {
@@ -416,8 +421,10 @@ __device__ __forceinline__ bool step_act(const DevParams& P, Photon& s, Rng& r, 
       // Readout face: interface to n_det, transmitted = detected; other faces:
       // interface to n_out, transmitted = escaped (transport.hpp:108-128).
       const bool readout = face == kReadoutFace;
-      const float n2 = readout ? P.n_det : P.n_out;
-      const float R = fresnel_R(P.n_scint, n2, readout ? P.eta2_det : P.eta2_out, cos_i);
+      const int oi = readout ? 0 : 1;
+      const float n2 = GP ? (&P.n_det)[oi] : (readout ? P.n_det : P.n_out);
+      const float R = fresnel_R(P.n_scint, n2, GP ? (&P.eta2_det)[oi] : (readout ? P.eta2_det : P.eta2_out),
+                                cos_i);
       k = 3u;
       if (r.uniform<2>() <= R) {
         flip = true;
@@ -428,7 +435,7 @@ __device__ __forceinline__ bool step_act(const DevParams& P, Photon& s, Rng& r, 
     } else if (model == kBlack) {
       fate = kAbsorbedSurface;
       live = false;
-    } else if (!(r.uniform<2>() <= face_refl(P, face))) {
+    } else if (!(r.uniform<2>() <= face_refl<GP>(P, face))) {
       // Painted reflector (transport.hpp:133-144): absorbed with 1 - R.
       fate = kAbsorbedSurface;
       live = false;
@@ -464,12 +471,12 @@ __device__ __forceinline__ bool step_act(const DevParams& P, Photon& s, Rng& r, 
 }
 
 // One step (transport.hpp:71-145): move, then interact.
-template <bool AUX>
+template <bool AUX, bool GP = false>
 __device__ __forceinline__ bool step_photon(const DevParams& P, Photon& s, Rng& r, uint64_t id,
                                             uint32_t& fate, ScoreAux& aux,
                                             uint32_t sync_mask = 0u) {
   const int hit = step_move(P, s, r);
-  return step_act<AUX>(P, s, r, id, fate, aux, hit, sync_mask);
+  return step_act<AUX, GP>(P, s, r, id, fate, aux, hit, sync_mask);
 }
 
 // Tally binning (transport.hpp:170-181); tscale = time_bins / time_max in float.

@@ -55,6 +55,8 @@ struct WaveArgs {
   uint32_t n_tallies;                   // events = tally slices (= n_events unless gensteps)
   uint32_t ev_shift;                    // ev_table resolution: one entry per 2^ev_shift photons
   uint32_t tail_steps;                  // steps a photon makes in a wave before it may be spilled at its end
+  uint32_t slot_cache;                  // batched tallies: 1 = warps may cache events in shared-memory
+                                        // slots (every record's max_steps < kSlotMaxAdd)
   const uint32_t* tally_of;             // record -> event (null: the record's own index)
   const float4* seg;                    // genstep records: 2 float4 each (end x,y,z,t0), (dt,-,-,-)
 };
@@ -90,10 +92,20 @@ constexpr uint32_t kEvShift = 7;  // coarsest event-table resolution: one entry 
 constexpr uint32_t kPantryBytesPerWarp = 32u * 112u;
 constexpr unsigned kErrQueue = 1u, kErrWatchdog = 2u;
 // Batched tallies: each warp caches the counters of two events in shared memory
-// (7 x u64 per event, padded to 8) and, when the tally has at most kSlotBins
-// histogram bins, their time / hit-map bins too (u32).
+// (7 x u32 per event, padded to 8) and, when the tally has at most kSlotBins
+// histogram bins, their time / hit-map bins too (u32). A warp flushes both its
+// slots to the events' u64 slices once kSlotFlushPhotons photons have entered it
+// since the last flush (checked at refills); events are cached only when every
+// record's max_steps is below kSlotMaxAdd (WaveArgs::slot_cache), so a photon
+// adds less than kSlotMaxAdd to a step sum. At most 64 more photons
+// (32 lanes, 32 in the pantry) can finish before the next check, so a u32
+// counter gains less than (kSlotFlushPhotons + 64) x kSlotMaxAdd < 2^32.
 constexpr uint32_t kSlotBins = 256u;
-constexpr uint32_t kSlotCounterBytesPerWarp = 2u * 8u * 8u;
+constexpr uint32_t kSlotCounterBytesPerWarp = 2u * 8u * 4u;
+constexpr uint32_t kSlotMaxAdd = 1u << 16;
+constexpr uint32_t kSlotFlushPhotons = 1u << 14;
+static_assert((static_cast<unsigned long long>(kSlotFlushPhotons) + 64u) * kSlotMaxAdd < (1ull << 32),
+              "slot counters must not wrap between flushes");
 inline __host__ __device__ uint32_t slot_bin_bytes_per_warp(uint32_t n_bins) {
   return n_bins <= kSlotBins ? 2u * n_bins * 4u : 0u;
 }

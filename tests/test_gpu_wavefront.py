@@ -84,6 +84,26 @@ def test_batched_events_exact_equals_oracle(engine, oracle):
         check_tally_consistency(row, c)
 
 
+@pytest.mark.parametrize("max_steps", [65_535, 65_536, 4_000_000_000])
+def test_batched_events_large_step_limits_equal_oracle(engine, oracle, max_steps):
+    """Warps cache events in shared-memory slots with 32-bit counters only when
+    every event's max_steps is below 2^16 (so one photon adds less than 2^16 to a
+    step sum); otherwise every photon adds to its event's 64-bit slice. Both
+    paths give the oracle's tallies (exact mode), with a long-lived photon mix
+    (mirror-like faces) so step sums are large."""
+    events, counts = batched_events(n_events=24, seed=31, median=5000, n_min=1, n_max=40000)
+    events = [e.replace(max_steps=max_steps, reflectivity=0.999, abs_length=20000.0) for e in events]
+    c = P.TallyConfig(100, 50.0, 10)
+    eng = WavefrontEngine(c, len(events), int(counts.sum()), WaveConfig(math="exact"))
+    eng.set_events(events, counts, first_id=77)
+    eng.run_tally()
+    got = eng.tallies()
+    eng.close()
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64) + np.uint64(77)
+    arr = (P.CSimParams * len(events))(*[e.to_c() for e in events])
+    assert np.array_equal(got, oracle.batch_tally(arr, offs, c, mode=oracle.PORTABLE))
+
+
 @pytest.mark.parametrize("math_mode", ["exact", "fast"])
 def test_batched_shared_physics_equals_oracle(engine, oracle, math_mode):
     """Events with the same step physics but their own sources, decay times and
