@@ -1097,11 +1097,10 @@ int optx_run_records(const optx_params* p, const optx_faces* faces, uint64_t n,
   return OPTX_OK;
 }
 
-// History tally grid: this many waves of resident blocks, each thread looping
-// over photons (grid-stride). Measured on B200 at 1e7 photons: 4 waves take
-// 2-4 % less time than 1 wave, and one photon per thread (as many blocks as
-// photons / block, each with its own histogram set-up and flush) 8-42 % more.
-constexpr uint64_t kHistoryGridWaves = 4;
+// History tally grid: one wave of resident blocks, each thread running its
+// photons one after another in one loop (history_loop). Measured on B200 at 1e7
+// photons: 1 wave takes 1-14 % less time than 4 waves with that loop.
+constexpr uint64_t kHistoryGridWaves = 1;
 
 int optx_run_tally(const optx_params* p, const optx_faces* faces, const optx_tally_config* c,
                    uint64_t n, uint64_t* tally_out, int block_size, uint64_t first_id, int math,

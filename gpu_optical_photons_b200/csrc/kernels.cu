@@ -5,7 +5,8 @@
 // source with --use_fast_math). Kernels:
 //
 //  * history_records_kernel / history_tally_kernel: one thread per photon for
-//    its whole history, the drop-in for the reference's transport_records_kernel
+//    its whole history (a thread runs its photons one after another in one
+//    loop, history_loop), the drop-in for the reference's transport_records_kernel
 //    and transport_tally_kernel (src/gpu/gpu_backend.cu:47-100 of the reference).
 //    The tally keeps fate counts and step sums in registers (no atomics) and the
 //    time / hit-map histograms in block-private shared memory, flushed once per
@@ -34,6 +35,8 @@
 //    kernel's bit for bit for any block size, threshold, cadence, chunk or wave size.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "optx_device.cuh"
 #include "optx_engine.hpp"
 
@@ -60,28 +63,52 @@ __device__ __forceinline__ void store_record(const DevRecords& out, uint64_t i, 
   out.path[i] = s.path;
 }
 
-// The full history of photon `id` (transport.hpp:151-159).
-template <bool AUX>
-__device__ __forceinline__ uint32_t transport(const DevParams& P, uint64_t id, Photon& s,
-                                              ScoreAux& aux) {
+// The histories of photons first_id + i for i = i0, i0 + stride, ... < n, one
+// after another in this thread (transport.hpp:151-159 per photon), in one loop
+// for all of them: a thread whose photon ended starts its next photon in the
+// next iteration instead of waiting, at the end of a per-photon loop, for the
+// longest history of its warp (measured: 1.7-2.2x on the single
+// configurations). Each photon's arithmetic is that of its own history, so
+// records and tallies do not depend on the grid. done(i, s, fate) is called
+// once per photon.
+template <class Done>
+__device__ __forceinline__ void history_loop(const DevParams& P, uint64_t first_id, uint64_t n,
+                                             uint64_t i, uint64_t stride, Done&& done) {
+  Photon s;
   Rng r;
-  r.init(id, P.key_lo, P.key_hi, 0u);
-  start_photon<AUX>(P, s, r, id, aux);
-  uint32_t fate = kMaxSteps;
-  for (uint32_t step = 0; step < P.max_steps; ++step) {
-    if (!step_photon<AUX>(P, s, r, id, fate, aux)) break;
+  ScoreAux aux{0u, 0.0f};
+  uint64_t cur = 0;
+  uint32_t step = 0;
+  bool alive = false;
+  for (;;) {
+    uint32_t fate = kMaxSteps;
+    bool ended;
+    if (!alive) {
+      if (i >= n) break;
+      cur = i;
+      i += stride;
+      const uint64_t id = first_id + cur;
+      r.init(id, P.key_lo, P.key_hi, 0u);
+      start_photon<false>(P, s, r, id, aux);
+      step = 0;
+      alive = true;
+      ended = P.max_steps == 0u;
+    } else {
+      ended = !step_photon<false>(P, s, r, first_id + cur, fate, aux);
+      if (!ended && ++step >= P.max_steps) ended = true;  // fate stays kMaxSteps
+    }
+    if (ended) {
+      alive = false;
+      done(cur, s, fate);
+    }
   }
-  return fate;
 }
 
 __global__ void history_records_kernel(const DevParams P, uint64_t first_id, uint64_t n,
                                        DevRecords out) {
-  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  Photon s;
-  ScoreAux aux{0u, 0.0f};
-  const uint32_t fate = transport<false>(P, first_id + i, s, aux);
-  store_record(out, i, s, fate);
+  history_loop(P, first_id, n, static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x,
+               static_cast<uint64_t>(gridDim.x) * blockDim.x,
+               [&](uint64_t i, const Photon& s, uint32_t fate) { store_record(out, i, s, fate); });
 }
 
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
@@ -109,24 +136,21 @@ __global__ void __launch_bounds__(1024, 1) history_tally_kernel(const DevParams 
 
   uint32_t f0 = 0, f1 = 0, f2 = 0, f3 = 0, f4 = 0;
   unsigned long long snb = 0, sns = 0;
-  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += stride) {
-    Photon s;
-    ScoreAux aux{0u, 0.0f};
-    const uint32_t fate = transport<false>(P, first_id + i, s, aux);
-    f0 += fate == 0u;
-    f1 += fate == 1u;
-    f2 += fate == 2u;
-    f3 += fate == 3u;
-    f4 += fate == 4u;
-    snb += s.nb;
-    sns += s.ns;
-    if (fate == kDetected) {
-      atomicAdd(&s_hist[time_bin(s.t, tc.tscale, tc.time_bins)], 1u);
-      atomicAdd(&s_hist[tc.time_bins + 1u + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins)], 1u);
-    }
-  }
+  history_loop(P, first_id, n, static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x,
+               static_cast<uint64_t>(gridDim.x) * blockDim.x,
+               [&](uint64_t, const Photon& s, uint32_t fate) {
+                 f0 += fate == 0u;
+                 f1 += fate == 1u;
+                 f2 += fate == 2u;
+                 f3 += fate == 3u;
+                 f4 += fate == 4u;
+                 snb += s.nb;
+                 sns += s.ns;
+                 if (fate == kDetected) {
+                   atomicAdd(&s_hist[time_bin(s.t, tc.tscale, tc.time_bins)], 1u);
+                   atomicAdd(&s_hist[tc.time_bins + 1u + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins)], 1u);
+                 }
+               });
   // Fates and sums: warp reductions, one global atomic per warp and counter.
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t r0 = __reduce_add_sync(kFull, f0), r1 = __reduce_add_sync(kFull, f1),
@@ -1037,7 +1061,14 @@ __global__ void __launch_bounds__(kSortThreads, MINB)
 cudaError_t launch_history_records(const DevParams& P, uint64_t first_id, uint64_t n,
                                    const DevRecords& out, int block, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
-  const uint64_t grid = (n + block - 1) / block;
+  // At most one wave of resident blocks: each thread runs several histories.
+  int dev = 0, sms = 1, bps = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, history_records_kernel, block, 0) != cudaSuccess ||
+      bps < 1)
+    bps = 1;
+  const uint64_t grid = std::min<uint64_t>((n + block - 1) / block, static_cast<uint64_t>(bps) * sms);
   history_records_kernel<<<static_cast<unsigned>(grid), block, 0, st>>>(P, first_id, n, out);
   return cudaGetLastError();
 }

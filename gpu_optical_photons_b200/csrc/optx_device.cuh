@@ -342,22 +342,25 @@ __device__ __forceinline__ int step_move(const DevParams& P, Photon& s, const Rn
 
   // Distance to the box exit: per axis only the face the photon moves towards
   // (geometry.hpp:25-46).
+  // All three quotients are computed and an axis the photon does not move along
+  // is then masked (its quotient, a division by zero, is never used): the same
+  // values as skipping it, without a branch per axis.
   float dist = kInf;
   int face = -1;
-  if (s.dx != 0.0f) {
+  {
     const bool pos = s.dx > 0.0f;
     const float tt = ((pos ? P.hx : -P.hx) - s.px) / s.dx;
-    if (tt < dist) { dist = tt; face = pos ? 1 : 0; }
+    if (s.dx != 0.0f && tt < dist) { dist = tt; face = pos ? 1 : 0; }
   }
-  if (s.dy != 0.0f) {
+  {
     const bool pos = s.dy > 0.0f;
     const float tt = ((pos ? P.hy : -P.hy) - s.py) / s.dy;
-    if (tt < dist) { dist = tt; face = pos ? 3 : 2; }
+    if (s.dy != 0.0f && tt < dist) { dist = tt; face = pos ? 3 : 2; }
   }
-  if (s.dz != 0.0f) {
+  {
     const bool pos = s.dz > 0.0f;
     const float tt = ((pos ? P.hz : -P.hz) - s.pz) / s.dz;
-    if (tt < dist) { dist = tt; face = pos ? 5 : 4; }
+    if (s.dz != 0.0f && tt < dist) { dist = tt; face = pos ? 5 : 4; }
   }
   dist = fmaxf(dist, 0.0f);
 
