@@ -111,6 +111,8 @@ _SIGS = {
     "optx_engine_destroy": [_P],
     "optx_engine_set_events": [_P, _P, _P, _P, ctypes.c_uint32, _u64, _P],
     "optx_engine_run_tally": [_P, _P],
+    "optx_engine_run_tally_range": [_P, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _P],
+    "optx_engine_set_tallies": [_P, _P, _P],
     "optx_engine_run_records": [_P, _P, _P],
     "optx_engine_run_adjoint": [_P, _P, ctypes.c_double, _P, _P],
     "optx_engine_run_score_moments": [_P, _P, _P],

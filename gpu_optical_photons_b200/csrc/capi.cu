@@ -416,6 +416,10 @@ struct optx_engine {
   bool gensteps = false;
   bool uniform = false;  // every event has the same step physics (see same_step_physics)
   uint64_t total = 0;              // photons of the batch (device gensteps: the capacity bound)
+  // The next run covers relative photons [run_lo, run_hi) and adds to the
+  // tallies when run_keep (optx_engine_run_tally_range); a plain run resets them.
+  uint64_t run_lo = 0, run_hi = 0;
+  bool run_range = false, run_keep = false;
   bool total_on_device = false;    // device gensteps: the run takes its total from d_offsets[n]
   uint64_t first_id = 0;
   DevParams P0{};
@@ -497,7 +501,9 @@ int engine_upload_args(optx_engine* e, int mode, int batch, int grid, cudaGraphC
   a.threshold = e->cfg.threshold;
   a.cadence = e->cfg.cadence;
   a.qcap = e->qcap;
-  a.total = e->total;
+  a.total = e->run_range ? e->run_hi : e->total;
+  a.item_lo = e->run_range ? e->run_lo : 0ull;
+  a.keep_tally = e->run_range && e->run_keep ? 1u : 0u;
   a.first_id = e->first_id;
   a.wave_quota = e->cfg.wave_quota ? e->cfg.wave_quota : (1ull << 31);
   if (a.wave_quota > (1ull << 30)) a.wave_quota = 1ull << 30;
@@ -1588,6 +1594,41 @@ int optx_engine_run_tally(optx_engine* e, void* stream) {
   if (e == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "engine must not be NULL");
   return engine_run(e, kModeTally, nullptr, nullptr, 0.0, nullptr, 0u,
                     static_cast<cudaStream_t>(stream));
+}
+
+int optx_engine_run_tally_range(optx_engine* e, uint64_t lo, uint64_t hi, int accumulate,
+                                void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "engine must not be NULL");
+  if (e->n_events == 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "no events uploaded");
+  if (e->total_on_device)
+    return fail(OPTX_ERR_INVALID_ARGUMENT,
+                "photon ranges need a photon total known on the host (not device gensteps)");
+  if (lo > hi || hi > e->total)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "photon range [" + std::to_string(lo) + ", " +
+                                               std::to_string(hi) + ") is not inside [0, " +
+                                               std::to_string(e->total) + "]");
+  e->run_range = true;
+  e->run_lo = lo;
+  e->run_hi = hi;
+  e->run_keep = accumulate != 0;
+  const int rc = engine_run(e, kModeTally, nullptr, nullptr, 0.0, nullptr, 0u,
+                            static_cast<cudaStream_t>(stream));
+  e->run_range = false;  // the arguments are on the device: later runs cover the whole batch
+  e->run_keep = false;
+  return rc;
+}
+
+int optx_engine_set_tallies(optx_engine* e, const uint64_t* host_tallies, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e == nullptr || host_tallies == nullptr)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "engine and host_tallies must not be NULL");
+  if (e->n_tallies == 0) return fail(OPTX_ERR_INVALID_ARGUMENT, "no events uploaded");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  OPTX_CUDA(cudaMemcpyAsync(e->d_tally, host_tallies, 8ull * e->tdev.len * e->n_tallies,
+                            cudaMemcpyHostToDevice, st));
+  OPTX_CUDA(cudaStreamSynchronize(st));
+  return OPTX_OK;
 }
 
 int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* stream) {

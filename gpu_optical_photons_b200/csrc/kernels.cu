@@ -215,9 +215,10 @@ __device__ __forceinline__ size_t qidx(uint32_t slot) {
 
 __global__ void wave_prep_kernel(const WaveArgs* __restrict__ A, WaveCtrl* __restrict__ ctrl) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    unsigned long long fresh = A->total < A->wave_quota ? A->total : A->wave_quota;
+    const unsigned long long lo = A->item_lo < A->total ? A->item_lo : A->total;
+    unsigned long long fresh = A->total - lo < A->wave_quota ? A->total - lo : A->wave_quota;
     if (A->cadence != 0u && fresh > A->qcap) fresh = A->qcap;
-    ctrl->fresh_next = 0ull;
+    ctrl->fresh_next = lo;
     ctrl->useful = 0ull;
     ctrl->issued = 0ull;
     ctrl->wave = 0u;
@@ -236,7 +237,7 @@ __global__ void wave_prep_kernel(const WaveArgs* __restrict__ A, WaveCtrl* __res
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nm; i += gridDim.x * blockDim.x)
       A->moments[i] = 0.0;
   }
-  if (A->tally != nullptr) {
+  if (A->tally != nullptr && A->keep_tally == 0u) {
     const size_t total = static_cast<size_t>(A->n_tallies) * A->tc.len;
     for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
          i += static_cast<size_t>(gridDim.x) * blockDim.x)

@@ -31,7 +31,8 @@ struct WaveArgs {
   uint32_t threshold;                   // refill a warp when fewer lanes than this are alive (1..32)
   uint32_t cadence;                     // steps per photon per wave before a forced spill (0 = none)
   uint32_t qcap;                        // capacity of each state queue, photons
-  unsigned long long total;             // photons in the run
+  unsigned long long total;             // the run covers relative photons [item_lo, total)
+  unsigned long long item_lo;           // first relative photon of the run (0: the whole batch)
   unsigned long long first_id;          // Philox id of relative photon 0
   unsigned long long wave_quota;        // fresh photons admitted per wave
   float4* qa;                           // state queues: tiles of 32 photons x 4 float4 (64 B each)
@@ -57,6 +58,7 @@ struct WaveArgs {
   uint32_t tail_steps;                  // steps a photon makes in a wave before it may be spilled at its end
   uint32_t slot_cache;                  // batched tallies: 1 = warps may cache events in shared-memory
                                         // slots (every record's max_steps < kSlotMaxAdd)
+  uint32_t keep_tally;                  // 1: the run adds to the tallies (no zeroing by the prep kernel)
   const uint32_t* tally_of;             // record -> event (null: the record's own index)
   const float4* seg;                    // genstep records: 2 float4 each (end x,y,z,t0), (dt,-,-,-)
 };

@@ -171,6 +171,21 @@ class WavefrontEngine:
         _lib.call("optx_engine_get_tallies", self._h, out.ctypes.data, ctypes.c_void_p(stream or 0))
         return out
 
+    def run_tally_range(self, lo: int, hi: int, accumulate: bool = True, stream=0):
+        """Transports the batch's relative photons [lo, hi) (photon i of event j
+        is offset_j + i) in tally mode, adding to the per-event tallies
+        (accumulate=True) or zeroing them first. Consecutive ranges give the
+        tallies of one whole run exactly: the unit of checkpoint and resume."""
+        _lib.call("optx_engine_run_tally_range", self._h, int(lo), int(hi), 1 if accumulate else 0,
+                  ctypes.c_void_p(stream or 0))
+
+    def set_tallies(self, tallies, stream=0):
+        """Replaces the per-event tallies (n_events x tally length) with host values."""
+        t = np.ascontiguousarray(tallies, dtype=np.uint64)
+        if t.shape != (self.n_events, self.tally_config.length):
+            raise ValueError(f"tallies must have shape ({self.n_events}, {self.tally_config.length})")
+        _lib.call("optx_engine_set_tallies", self._h, t.ctypes.data, ctypes.c_void_p(stream or 0))
+
     def tally_ptr(self):
         p = ctypes.c_void_p()
         ln = ctypes.c_uint64()
@@ -257,6 +272,70 @@ class SortedEngine:
         st = _lib.CSortedCounters()
         _lib.call("optx_sorted_stats", self._h, ctypes.byref(st), _stream_ptr(stream))
         return st.as_dict()
+
+
+# ---- checkpoint and resume of a batched run ---------------------------------
+
+def batch_fingerprint(events, counts, first_id: int, tally: TallyConfig) -> str:
+    """SHA-256 over the batch's C parameter records, photon counts, first id and
+    tally binning: a checkpoint resumes only the batch it was taken from."""
+    import hashlib
+    arr, faces = _events_c(events)
+    h = hashlib.sha256()
+    h.update(bytes(arr))
+    if faces is not None:
+        h.update(bytes(faces))
+    h.update(np.ascontiguousarray(counts, dtype=np.uint64).tobytes())
+    h.update(np.uint64(first_id).tobytes())
+    h.update(np.array([tally.time_bins, tally.xy_bins], np.uint32).tobytes())
+    h.update(np.float32(tally.time_max).tobytes())
+    return h.hexdigest()
+
+
+def save_checkpoint(path: str, fingerprint: str, next_index: int, tallies) -> None:
+    """Writes a checkpoint (.npz): the batch fingerprint, the next relative photon
+    index and the per-event tallies so far."""
+    np.savez(path, fingerprint=np.array(fingerprint), next_index=np.uint64(next_index),
+             tallies=np.ascontiguousarray(tallies, dtype=np.uint64))
+
+
+def load_checkpoint(path: str, fingerprint: str):
+    """(next relative photon index, tallies) of a checkpoint taken from the batch
+    with this fingerprint; ValueError for another batch."""
+    with np.load(path) as z:
+        if str(z["fingerprint"]) != fingerprint:
+            raise ValueError("the checkpoint was taken from another batch (events, counts, "
+                             "first_id or tally binning differ)")
+        return int(z["next_index"]), z["tallies"].copy()
+
+
+def run_tally_checkpointed(engine: "WavefrontEngine", events, counts, first_id: int = 0,
+                           path: str | None = None, slice_photons: int = 1 << 24,
+                           stop_after: int | None = None):
+    """Runs the uploaded batch in slices of `slice_photons` photons, writing a
+    checkpoint to `path` after each slice, and resumes from `path` when it
+    holds a checkpoint of this batch. `stop_after` ends the call after that
+    many slices (an interrupted run). Returns (tallies, next index); the run is
+    complete when the next index equals the batch's photon total."""
+    import os
+    total = int(np.asarray(counts, dtype=np.uint64).sum())
+    fp = batch_fingerprint(events, counts, first_id, engine.tally_config)
+    start = 0
+    if path is not None and os.path.exists(path):
+        start, t = load_checkpoint(path, fp)
+        engine.set_tallies(t)
+    done = 0
+    lo = start
+    while lo < total and (stop_after is None or done < stop_after):
+        hi = min(total, lo + slice_photons)
+        engine.run_tally_range(lo, hi, accumulate=lo > 0)
+        lo = hi
+        done += 1
+        if path is not None:
+            save_checkpoint(path, fp, lo, engine.tallies())
+    if total == 0:
+        engine.run_tally()
+    return engine.tallies(), lo
 
 
 def wavefront_tally(p: SimParams, c: TallyConfig, n: int, first_id: int = 0,

@@ -270,6 +270,25 @@ int optx_engine_set_gensteps_device(optx_engine* e, const optx_params* events,
 /* Runs the uploaded batch; per-event tallies stay on the device (overwritten).
  * Asynchronous on `stream`. */
 int optx_engine_run_tally(optx_engine* e, void* stream);
+/* Checkpoint and resume of a batched run (the batch's counterpart of the
+ * reference's restartable runs: first_id in backend.hpp:84-115 and a Philox
+ * stream resumed from its draws, philox.hpp:117-134). Photon i of event j has
+ * the relative index offset_j + i (offsets = prefix sums of the counts); a
+ * photon's history depends only on (seed, first_id + relative index), so a batch
+ * run as consecutive ranges [0, a), [a, b), ... gives the uninterrupted run's
+ * tallies exactly. optx_engine_run_tally_range transports the relative photons
+ * [lo, hi) in tally mode, async on `stream`; accumulate = 0 zeroes the per-event
+ * tallies first (as optx_engine_run_tally does), 1 adds to them. A checkpoint is
+ * (the batch, the next relative index, the tallies from
+ * optx_engine_get_tallies); to resume — in this process or another — upload the
+ * same batch with the same first_id, restore the tallies with
+ * optx_engine_set_tallies, and continue with accumulate = 1. Not available after
+ * optx_engine_set_gensteps_device (the photon total lives on the device). */
+int optx_engine_run_tally_range(optx_engine* e, uint64_t lo, uint64_t hi, int accumulate,
+                                void* stream);
+/* Replaces the per-event tallies (n_events x tally length u64, host memory),
+ * e.g. with a checkpoint's; synchronous on `stream`. */
+int optx_engine_set_tallies(optx_engine* e, const uint64_t* host_tallies, void* stream);
 /* Runs the uploaded batch writing records (device arrays indexed by photon
  * index relative to first_id, total entries = sum of counts). */
 int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* stream);
