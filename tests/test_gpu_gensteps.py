@@ -246,3 +246,24 @@ def _lib_call_too_many(eng, events):
     dummy = torch.zeros(40, dtype=torch.uint8, device="cuda")
     _lib.call("optx_engine_set_gensteps_device", eng._h, ctypes.cast(arr, ctypes.c_void_p), None,
               len(events), ctypes.c_void_p(dummy.data_ptr()), eng.config.max_gensteps + 1, 0, None)
+
+
+def test_genstep_ranges_equal_one_run(engine, oracle):
+    """A genstep batch run as photon ranges (checkpoint and resume) gives the
+    one-run tallies; ranges are refused after a device-genstep upload, whose
+    photon total the host does not know."""
+    events, g = _workload(seed=9)
+    n = G.photons_of(g)
+    eng = _engine(events, g)
+    try:
+        eng.set_gensteps(events, g, first_id=55)
+        for i, (lo, hi) in enumerate([(0, n // 5), (n // 5, n // 2), (n // 2, n)]):
+            eng.run_tally_range(lo, hi, accumulate=i > 0)
+        got = eng.tallies()
+        ref, _ = oracle.genstep_run(events, g, TC, first_id=55, mode=oracle.PORTABLE)
+        assert np.array_equal(got, ref)
+        eng.set_gensteps_device(events, G.to_device(g), first_id=55)
+        with pytest.raises(InvalidArgument, match="photon ranges"):
+            eng.run_tally_range(0, 10)
+    finally:
+        eng.close()
