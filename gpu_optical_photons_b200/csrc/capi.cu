@@ -473,7 +473,7 @@ int engine_grid(optx_engine* e, int mode, int batch, int& grid) {
   if (smem > static_cast<size_t>(max_smem))
     return fail(OPTX_ERR_RUNTIME, "wavefront kernel needs " + std::to_string(smem) +
                                       " bytes of shared memory per block; reduce xy_bins / time_bins");
-  if (smem > 48 * 1024) OPTX_CUDA(DISPATCH(math, wave_set_smem, mode, batch, minb, smem));
+  if (smem > kDynSmemOptIn) OPTX_CUDA(DISPATCH(math, wave_set_smem, mode, batch, minb, smem));
   int bps = DISPATCH(math, wave_blocks_per_sm, mode, batch, minb, e->cfg.block_size, smem);
   if (bps <= 0) return fail(OPTX_ERR_RUNTIME, "wavefront kernel cannot be resident with this block size / tally");
   if (e->cfg.blocks_per_sm == 7) bps = std::min(bps, 7);
@@ -2157,7 +2157,7 @@ extern "C" int optx_wavefront_tally_noalloc(const optx_params* p, const optx_fac
   const DevParams P = make_dev_params(*p, faces);
   const size_t smem = static_cast<size_t>(kBlock / 32) * kPantryBytesPerWarp +
                       static_cast<size_t>(td.len - 7u) * 4u;
-  if (smem > 48 * 1024) OPTX_CUDA(DISPATCH(math, wave_set_smem, kModeTally, kSingle, kMinB, smem));
+  if (smem > kDynSmemOptIn) OPTX_CUDA(DISPATCH(math, wave_set_smem, kModeTally, kSingle, kMinB, smem));
   const int bps = DISPATCH(math, wave_blocks_per_sm, kModeTally, kSingle, kMinB, kBlock, smem);
   if (bps <= 0)
     return fail(OPTX_ERR_RUNTIME, "tally histograms need too much shared memory; reduce xy_bins / time_bins");

@@ -1088,7 +1088,7 @@ cudaError_t launch_history_tally(const DevParams& P, const TallyDev& tc, uint64_
                                  uint64_t n, unsigned long long* tally, int block, int grid,
                                  cudaStream_t st) {
   const size_t smem = static_cast<size_t>(tc.len - 7u) * sizeof(uint32_t);
-  if (smem > 48 * 1024) {
+  if (smem > kDynSmemOptIn) {
     const cudaError_t e = cudaFuncSetAttribute(
         history_tally_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;

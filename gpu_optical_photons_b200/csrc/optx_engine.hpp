@@ -92,6 +92,10 @@ constexpr uint32_t kEvShift = 7;  // coarsest event-table resolution: one entry 
 // Shared memory of one warp's pantry: 32 ready photons x 112 bytes (7 x 16 B;
 // the 112-byte stride makes 8 lanes' 128-bit accesses hit 8 distinct bank groups).
 constexpr uint32_t kPantryBytesPerWarp = 32u * 112u;
+// Dynamic shared memory above this needs the kernel's opt-in attribute: the
+// default limit is 48 KB minus the kernel's static shared memory (at most 1 KB
+// for the kernels here).
+constexpr size_t kDynSmemOptIn = 47u * 1024u;
 constexpr unsigned kErrQueue = 1u, kErrWatchdog = 2u;
 // Batched tallies: each warp caches the counters of two events in shared memory
 // (7 x u32 per event, padded to 8) and, when the tally has at most kSlotBins

@@ -201,3 +201,22 @@ def test_run_batch_with_event_table(engine):
     finally:
         eng.close()
     assert np.array_equal(a, b) and np.array_equal(a, c)
+
+
+def test_tally_just_under_the_default_shared_memory_limit(engine, oracle):
+    """A tally whose histograms bring the wave kernel's dynamic shared memory to
+    49,072 B: below 48 KB, but above 48 KB minus the kernel's static shared memory,
+    so the launch needs the opt-in attribute all the same."""
+    p = P.config2()[0]
+    c = P.TallyConfig(5098, 50.0, 1)  # 5 + 5099 + 1 + 2 entries; bins 5100 x 4 B + 8 pantries x 3584 B
+    n = 100_000
+    want = oracle.tally(p, c, n, 9, mode=oracle.PORTABLE)
+    eng = WavefrontEngine(c, 1, n, WaveConfig(math="exact"))
+    try:
+        eng.set_events([p], [n], first_id=9)
+        eng.run_tally()
+        assert np.array_equal(eng.tallies()[0], want)
+    finally:
+        eng.close()
+    _, flat, _ = engine.run_gpu_tally(p, c, n, first_id=9, math="exact")
+    assert np.array_equal(flat, want)
