@@ -470,9 +470,13 @@ int engine_grid(optx_engine* e, int mode, int batch, int& grid) {
   int dev = 0, max_smem = 0;
   OPTX_CUDA(cudaGetDevice(&dev));
   OPTX_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  if (smem > static_cast<size_t>(max_smem))
-    return fail(OPTX_ERR_RUNTIME, "wavefront kernel needs " + std::to_string(smem) +
-                                      " bytes of shared memory per block; reduce xy_bins / time_bins");
+  // The opt-in maximum covers the kernel's static shared memory too.
+  cudaFuncAttributes fa{};
+  OPTX_CUDA(cudaFuncGetAttributes(&fa, DISPATCH(math, wave_kernel_fn, mode, batch, minb)));
+  if (smem + fa.sharedSizeBytes > static_cast<size_t>(max_smem))
+    return fail(OPTX_ERR_RUNTIME, "wavefront kernel needs " + std::to_string(smem + fa.sharedSizeBytes) +
+                                      " bytes of shared memory per block (" + std::to_string(max_smem) +
+                                      " available); reduce xy_bins / time_bins");
   if (smem > kDynSmemOptIn) OPTX_CUDA(DISPATCH(math, wave_set_smem, mode, batch, minb, smem));
   int bps = DISPATCH(math, wave_blocks_per_sm, mode, batch, minb, e->cfg.block_size, smem);
   if (bps <= 0) return fail(OPTX_ERR_RUNTIME, "wavefront kernel cannot be resident with this block size / tally");

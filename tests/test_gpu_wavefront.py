@@ -220,3 +220,20 @@ def test_tally_just_under_the_default_shared_memory_limit(engine, oracle):
         eng.close()
     _, flat, _ = engine.run_gpu_tally(p, c, n, first_id=9, math="exact")
     assert np.array_equal(flat, want)
+
+
+def test_tally_at_the_top_of_shared_memory(engine, oracle):
+    """Histograms that fit the opt-in shared memory per block beside the pantries
+    of 8 warps only if the kernel's static shared memory is forgotten: the engine
+    refuses them with a clear error (no CUDA error), and the host tally call still
+    answers, bit for bit (history kernel or the 4-warp engine of the host calls)."""
+    import torch
+    props = torch.cuda.get_device_properties(0)
+    optin = int(getattr(props, "shared_memory_per_block_optin", 232448))
+    n_bins = (optin - 8 * 3584) // 4 - 6  # dynamic bytes within the kernel's static size of the limit
+    c = P.TallyConfig(n_bins - 2, 50.0, 1)  # time bins + overflow + 1 hit-map bin = n_bins
+    with pytest.raises(engine.OptxError, match="shared memory"):
+        WavefrontEngine(c, 1, 1000, WaveConfig(math="exact"))
+    p = P.config1()[0]
+    _, flat, _ = engine.run_gpu_tally(p, c, 20_000, first_id=3, math="exact")
+    assert np.array_equal(flat, oracle.tally(p, c, 20_000, 3, mode=oracle.PORTABLE))
