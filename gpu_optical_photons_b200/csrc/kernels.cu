@@ -77,6 +77,23 @@ __device__ __forceinline__ void history_loop(const DevParams& P, uint64_t first_
   Photon s;
   Rng r;
   ScoreAux aux{0u, 0.0f};
+  // At most one photon for this thread (a launch that covers its photons in one
+  // grid pass, e.g. one event of a batch): the plain per-photon loop, which is
+  // tighter (measured: 4096 per-event launches 229 -> 182 ms; +1 % on 1e7-photon
+  // launches, where threads run several photons through the single loop).
+  if (i + stride >= n) {
+    if (i < n) {
+      const uint64_t id = first_id + i;
+      r.init(id, P.key_lo, P.key_hi, 0u);
+      start_photon<false>(P, s, r, id, aux);
+      uint32_t fate = kMaxSteps;
+      for (uint32_t st = 0; st < P.max_steps; ++st) {
+        if (!step_photon<false>(P, s, r, id, fate, aux)) break;
+      }
+      done(i, s, fate);
+    }
+    return;
+  }
   uint64_t cur = 0;
   uint32_t step = 0;
   bool alive = false;
@@ -104,7 +121,8 @@ __device__ __forceinline__ void history_loop(const DevParams& P, uint64_t first_
   }
 }
 
-__global__ void history_records_kernel(const DevParams P, uint64_t first_id, uint64_t n,
+// Blocks of up to 1024 threads (the accepted block sizes): at most 64 registers.
+__global__ void __launch_bounds__(1024, 1) history_records_kernel(const DevParams P, uint64_t first_id, uint64_t n,
                                        DevRecords out) {
   history_loop(P, first_id, n, static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x,
                static_cast<uint64_t>(gridDim.x) * blockDim.x,

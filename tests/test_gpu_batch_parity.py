@@ -7,7 +7,7 @@ absorption, reflectivity, refractive index and scattering; Lambertian cube;
   the reference's OPTPHOT_PORTABLE_MATH CPU build), for the engine settings the
   benchmark runs (7 blocks of 128 threads, the 72-register budget), the default
   settings, and the plain history kernel launched once per event.
-* Fast mode: against the oracle's default-math CPU run of the same photons, the
+* Fast and approx modes: against the oracle's default-math CPU run of the same photons, the
   detected counts differ by <= 1e-3 of the photons, the per-event fate counts by
   <= 1e-3 in total, and the summed arrival-time histogram and hit map pass the
   two-sample chi-squared test (p > 0.01); on the first 64 events the per-photon
@@ -66,11 +66,18 @@ def test_full_batch_exact_equals_oracle(engine, oracle, batch):
     assert np.array_equal(hist, want)
 
 
-def test_full_batch_fast_agrees_with_cpu(engine, oracle, batch):
+@pytest.fixture(scope="module")
+def cpu_platform(oracle, batch):
+    events, counts, offs, arr = batch
+    return oracle.batch_tally(arr, offs, TC, mode=oracle.PLATFORM)
+
+
+@pytest.mark.parametrize("math_mode", ["fast", "approx"])
+def test_full_batch_fast_agrees_with_cpu(engine, oracle, batch, cpu_platform, math_mode):
     events, counts, offs, arr = batch
     n = int(counts.sum())
-    want = oracle.batch_tally(arr, offs, TC, mode=oracle.PLATFORM)
-    got, _ = engine_tallies(events, counts, WaveConfig(math="fast", blocks_per_sm=7, block_size=128))
+    want = cpu_platform
+    got, _ = engine_tallies(events, counts, WaveConfig(math=math_mode, blocks_per_sm=7, block_size=128))
     assert int(got[:, :5].sum()) == n
     # Detected photons: |sum over events of the difference| and the sum of
     # per-event |differences|, both within the 0.1 % fate tolerance.
@@ -90,7 +97,7 @@ def test_full_batch_fast_agrees_with_cpu(engine, oracle, batch):
     from gpu_optical_photons_b200.backend import device_records, records_to_numpy
     k = 64
     m = int(offs[k])
-    eng = WavefrontEngine(TC, k, m, WaveConfig(math="fast", blocks_per_sm=7, block_size=128))
+    eng = WavefrontEngine(TC, k, m, WaveConfig(math=math_mode, blocks_per_sm=7, block_size=128))
     try:
         eng.set_events(events[:k], counts[:k])
         d = device_records(m)
