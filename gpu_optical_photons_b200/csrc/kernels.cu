@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
   // Warp-uniform bookkeeping: the work items [chunk_lo, chunk_hi) claimed by this
   // warp and not yet emitted; batched, the events cached in its two shared-memory
   // slots and the slot replaced next. Batched variants keep these in shared
-  // memory (measured: fewer local-memory spills, -5 % per photon-step on the
+  // memory (measured: fewer local-memory spills, -2.5 % per photon-step on the
   // batch), the single-configuration ones in registers.
   constexpr uint32_t kNoEvent = 0xffffffffu;
   // [warp][chunk_lo, chunk_hi, tag0, tag1, victim, photons since the last slot flush]
@@ -437,8 +437,8 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
       store_record(A->rec, pidx, s, fate);
     } else if (MODE == kModeTally && BATCH) {
       // 32-bit shared-memory atomics into the event's slot when the warp caches
-      // it (a 64-bit shared add costs a compare-and-swap loop: measured -10 % per
-      // photon-step on the batch), else 64-bit global atomics into the event's
+      // it (a 64-bit shared-memory add is not one atomic instruction: u64 slots
+      // measured +10 % per photon-step on the batch), else 64-bit global atomics into the event's
       // slice. Events are cached only when every record's max_steps is below
       // kSlotMaxAdd (so is each photon's nb and ns), and the warp flushes its
       // slots every kSlotFlushPhotons photons (at a refill): no u32 counter wraps.
