@@ -27,6 +27,7 @@
 //    are computed with the same float operations as the reference.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -54,6 +55,16 @@ struct __align__(16) DevParams {
   uint32_t key_hi, pad0, pad1, pad2;
 };
 static_assert(sizeof(DevParams) == 112, "DevParams layout");
+// Indexed reads of a record in global memory (face_refl, step_act) rely on these
+// runs of consecutive floats: refl0..refl4, (n_det, n_out), (eta2_det, eta2_out).
+static_assert(offsetof(DevParams, refl1) == offsetof(DevParams, refl0) + 4 &&
+                  offsetof(DevParams, refl2) == offsetof(DevParams, refl0) + 8 &&
+                  offsetof(DevParams, refl3) == offsetof(DevParams, refl0) + 12 &&
+                  offsetof(DevParams, refl4) == offsetof(DevParams, refl0) + 16,
+              "DevParams reflectivities must be consecutive");
+static_assert(offsetof(DevParams, n_out) == offsetof(DevParams, n_det) + 4 &&
+                  offsetof(DevParams, eta2_out) == offsetof(DevParams, eta2_det) + 4,
+              "DevParams readout / outside pairs must be consecutive");
 
 // Device-side structure-of-arrays photon records (29 bytes per photon).
 struct DevRecords {
