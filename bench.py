@@ -217,6 +217,28 @@ def chi2_two_sample(a, b):
     return chi2, ndf, float(ss.chi2.sf(chi2, ndf)) if ndf > 0 else 1.0
 
 
+def tally_parity(gpu_tallies, cpu_tallies, tc) -> dict:
+    """Per-event tallies of the same photons from the GPU and the CPU (rows 0 ..
+    len(cpu_tallies) - 1): detected counts, fate-count changes (at least
+    sum |delta| / 2 photons changed fate) and the two-sample chi-squared p of the
+    summed arrival-time histogram and hit map."""
+    ne = len(cpu_tallies)
+    g = np.asarray(gpu_tallies[:ne], np.uint64)
+    c = np.asarray(cpu_tallies, np.uint64)
+    photons = int(c[:, :5].sum())
+    d_det = g[:, 0].astype(np.int64) - c[:, 0].astype(np.int64)
+    d_fates = int(np.abs(g[:, :5].astype(np.int64) - c[:, :5].astype(np.int64)).sum())
+    t0, x0 = 5, 5 + tc.time_bins + 1
+    _, _, p_time = chi2_two_sample(g[:, t0:x0].sum(axis=0), c[:, t0:x0].sum(axis=0))
+    _, _, p_hit = chi2_two_sample(g[:, x0:x0 + tc.xy_bins ** 2].sum(axis=0), c[:, x0:x0 + tc.xy_bins ** 2].sum(axis=0))
+    return {"events": ne, "photons": photons,
+            "detected_gpu": int(g[:, 0].sum()), "detected_cpu": int(c[:, 0].sum()),
+            "abs_delta_detected_over_photons": int(np.abs(d_det).sum()) / photons,
+            "fate_count_changes_lower_bound_frac": d_fates / 2 / photons,
+            "chi2_p_time_hist": p_time, "chi2_p_hit_map": p_hit,
+            "total_photons_equal": int(g[:, :5].sum()) == photons}
+
+
 def parity_leg(gpu_tallies, cpu_tallies, events, counts, tc, cfg, math: str, k_records: int = 64) -> dict:
     """The benchmarked batch against the reference CPU run of the same photons.
 
@@ -230,22 +252,9 @@ def parity_leg(gpu_tallies, cpu_tallies, events, counts, tc, cfg, math: str, k_r
     from oracle import oracle as O
     from gpu_optical_photons_b200.backend import device_records, records_to_numpy
     from gpu_optical_photons_b200.wavefront import WavefrontEngine
-    ne = len(cpu_tallies)
-    g = np.asarray(gpu_tallies[:ne], np.uint64)
-    c = np.asarray(cpu_tallies, np.uint64)
-    photons = int(c[:, :5].sum())
-    d_det = g[:, 0].astype(np.int64) - c[:, 0].astype(np.int64)
-    d_fates = int(np.abs(g[:, :5].astype(np.int64) - c[:, :5].astype(np.int64)).sum())
-    t0, x0 = 5, 5 + tc.time_bins + 1
-    _, _, p_time = chi2_two_sample(g[:, t0:x0].sum(axis=0), c[:, t0:x0].sum(axis=0))
-    _, _, p_hit = chi2_two_sample(g[:, x0:x0 + tc.xy_bins ** 2].sum(axis=0), c[:, x0:x0 + tc.xy_bins ** 2].sum(axis=0))
-    out = {"events": ne, "photons": photons, "gpu_math": math,
-           "cpu": "reference run_cpu_tally (default build)" if O.ref_available() else "oracle port (default math)",
-           "detected_gpu": int(g[:, 0].sum()), "detected_cpu": int(c[:, 0].sum()),
-           "abs_delta_detected_over_photons": int(np.abs(d_det).sum()) / photons,
-           "fate_count_changes_lower_bound_frac": d_fates / 2 / photons,
-           "chi2_p_time_hist": p_time, "chi2_p_hit_map": p_hit,
-           "total_photons_equal": int(g[:, :5].sum()) == photons}
+    out = {**tally_parity(gpu_tallies, cpu_tallies, tc), "gpu_math": math,
+           "cpu": "reference run_cpu_tally (default build)" if O.ref_available() else "oracle port (default math)"}
+    p_time, p_hit = out["chi2_p_time_hist"], out["chi2_p_hit_map"]
     offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
     k = min(k_records, len(events))
     m = int(offs[k])

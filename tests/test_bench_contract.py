@@ -38,3 +38,40 @@ def test_reference_arm_other_ranks_exit_quietly():
     out = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert out.returncode == 0, out.stderr[-2000:]
     assert not [l for l in out.stdout.splitlines() if l.startswith("{")]
+
+
+def test_tally_parity_metrics():
+    """bench.py's parity metrics on planted tallies (CPU): equal tallies give no
+    differences and p = 1; photons moved from detected to absorbed show up as
+    detection and fate-count differences; a shifted arrival-time histogram fails
+    the chi-squared test."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    import bench
+    from gpu_optical_photons_b200 import params as P
+    tc = P.TallyConfig(20, 50.0, 2)
+    rng = np.random.default_rng(1)
+    cpu = np.zeros((6, tc.length), np.uint64)
+    for row in cpu:
+        fates = rng.multinomial(10_000, [0.6, 0.2, 0.2, 0.0, 0.0])
+        row[:5] = fates
+        row[5:5 + 21] = rng.multinomial(int(fates[0]), [1 / 21] * 21)
+        row[26:30] = rng.multinomial(int(fates[0]), [0.25] * 4)
+    same = bench.tally_parity(cpu.copy(), cpu, tc)
+    assert same["photons"] == 60_000 and same["total_photons_equal"]
+    assert same["abs_delta_detected_over_photons"] == 0 and same["fate_count_changes_lower_bound_frac"] == 0
+    assert same["chi2_p_time_hist"] == pytest.approx(1.0) and same["chi2_p_hit_map"] == pytest.approx(1.0)
+    moved = cpu.copy()
+    moved[0, 0] -= 30
+    moved[0, 1] += 30
+    moved[0, 5] -= 30  # those photons leave the time histogram and the hit map
+    moved[0, 26] -= 30
+    d = bench.tally_parity(moved, cpu, tc)
+    assert d["abs_delta_detected_over_photons"] == pytest.approx(30 / 60_000)
+    assert d["fate_count_changes_lower_bound_frac"] == pytest.approx(30 / 60_000)
+    assert d["total_photons_equal"]
+    shifted = cpu.copy()
+    moved_n = np.minimum(shifted[:, 6], 200)  # photons of the second time bin ...
+    shifted[:, 6] -= moved_n
+    shifted[:, 5] += moved_n                   # ... counted in the first
+    assert bench.tally_parity(shifted, cpu, tc)["chi2_p_time_hist"] < 0.01
