@@ -137,6 +137,11 @@ DevParams make_dev_params(const optx_params& p, const optx_faces* f) {
   d.eta2_out = e2 * e2;
   d.key_lo = static_cast<uint32_t>(p.seed);
   d.key_hi = static_cast<uint32_t>(p.seed >> 32);
+  // Reciprocals for the hit-map binning (xy_bin): float divisions, correctly
+  // rounded (2 hx is exact).
+  volatile float two_hx = 2.0f * p.hx, two_hy = 2.0f * p.hy;
+  d.inv2hx = 1.0f / two_hx;
+  d.inv2hy = 1.0f / two_hy;
   return d;
 }
 
@@ -1385,7 +1390,7 @@ static bool same_step_physics(DevParams a, DevParams b) {
     d->tau = 0.0f;
     d->src_x = d->src_y = d->src_z = 0.0f;
     d->source = 0u;
-    d->pad0 = d->pad1 = d->pad2 = 0u;
+    d->pad2 = 0u;
   }
   return std::memcmp(&a, &b, sizeof(DevParams)) == 0;
 }

@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(1024, 1) history_tally_kernel(const DevParams 
                  sns += s.ns;
                  if (fate == kDetected) {
                    atomicAdd(&s_hist[time_bin(s.t, tc.tscale, tc.time_bins)], 1u);
-                   atomicAdd(&s_hist[tc.time_bins + 1u + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins)], 1u);
+                   atomicAdd(&s_hist[tc.time_bins + 1u + xy_bin(s.px, s.py, P, tc.xy_bins)], 1u);
                  }
                });
   // Fates and sums: warp reductions, one global atomic per warp and counter.
@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
       }
       if (fate == kDetected) {
         const uint32_t tb = time_bin(s.t, tc.tscale, tc.time_bins);
-        const uint32_t xb = tc.time_bins + 1u + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins);
+        const uint32_t xb = tc.time_bins + 1u + xy_bin(s.px, s.py, P, tc.xy_bins);
         if (slot >= 0 && slot_bins) {
           uint32_t* sb = s_sb + static_cast<uint32_t>(slot) * n_bins;
           atomicAdd(&sb[tb], 1u);
@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(wave_max_threads<MINB>(), MINB) wave_kernel(co
       sns += s.ns;
       if (fate == kDetected) {
         atomicAdd(&s_hist[time_bin(s.t, tc.tscale, tc.time_bins)], 1u);
-        atomicAdd(&s_hist[tc.time_bins + 1u + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins)], 1u);
+        atomicAdd(&s_hist[tc.time_bins + 1u + xy_bin(s.px, s.py, P, tc.xy_bins)], 1u);
       }
     } else {  // adjoint: score terms of detected photons (see WaveArgs)
       if (fate == kDetected) {
@@ -1009,7 +1009,7 @@ __global__ void __launch_bounds__(kSortThreads, MINB)
       sns += s.ns;
       if (fate == kDetected && tally != nullptr) {
         atomicAdd(tally + 5u + time_bin(s.t, tc.tscale, tc.time_bins), 1ull);
-        atomicAdd(tally + 6u + tc.time_bins + xy_bin(s.px, s.py, P.hx, P.hy, tc.xy_bins), 1ull);
+        atomicAdd(tally + 6u + tc.time_bins + xy_bin(s.px, s.py, P, tc.xy_bins), 1ull);
       }
     }
   }

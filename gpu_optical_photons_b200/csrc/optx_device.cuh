@@ -52,7 +52,9 @@ struct __align__(16) DevParams {
   float refl0, refl1, refl2, refl3;        // reflectivity of faces 0..4
   float refl4, eta2_det, eta2_out;         // (n_scint/n_det)^2, (n_scint/n_out)^2 (fresnel.hpp:32-33)
   uint32_t key_lo;
-  uint32_t key_hi, pad0, pad1, pad2;
+  uint32_t key_hi;
+  float inv2hx, inv2hy;                    // 1 / (2 hx), 1 / (2 hy) rounded to nearest (xy_bin)
+  uint32_t pad2;
 };
 static_assert(sizeof(DevParams) == 112, "DevParams layout");
 // Indexed reads of a record in global memory (face_refl, step_act) rely on these
@@ -502,10 +504,23 @@ __device__ __forceinline__ uint32_t time_bin(float t, float tscale, uint32_t tim
   const float f = t * tscale;
   return (f >= static_cast<float>(time_bins)) ? time_bins : static_cast<uint32_t>(f);
 }
-__device__ __forceinline__ uint32_t xy_bin(float x, float y, float hx, float hy, uint32_t xy_bins) {
+// a / b for 0 <= a <= b from y = 1 / b rounded to nearest: the product and two
+// FMA corrections. With y the correctly rounded reciprocal and q1 within an ulp
+// of a / b, q1 + (a - b q1) y rounds to the correctly rounded quotient
+// (Markstein, IBM J. Res. Dev. 34(1), 1990), so this equals the IEEE division
+// a / b whenever a / b does not underflow; checked on B200 against __fdiv_rn
+// for every a in [b 2^-100, b] of several divisors and for random (a, b) pairs
+// (tests/test_gpu_quotient.py). Here a / b >= 2^-25 or a = 0 (a = x + hx with
+// |x| <= hx). Measured: -0.8 % per photon-step on the batch (FAST), -1.6 % (EXACT).
+__device__ __forceinline__ float quot_rn(float a, float b, float y) {
+  const float q0 = a * y;
+  const float q1 = fmaf(fmaf(-q0, b, a), y, q0);
+  return fmaf(fmaf(-q1, b, a), y, q1);
+}
+__device__ __forceinline__ uint32_t xy_bin(float x, float y, const DevParams& P, uint32_t xy_bins) {
   const float nbf = static_cast<float>(xy_bins);
-  const uint32_t ix = static_cast<uint32_t>(fminf((x + hx) / (2.0f * hx) * nbf, nbf - 1.0f));
-  const uint32_t iy = static_cast<uint32_t>(fminf((y + hy) / (2.0f * hy) * nbf, nbf - 1.0f));
+  const uint32_t ix = static_cast<uint32_t>(fminf(quot_rn(x + P.hx, 2.0f * P.hx, P.inv2hx) * nbf, nbf - 1.0f));
+  const uint32_t iy = static_cast<uint32_t>(fminf(quot_rn(y + P.hy, 2.0f * P.hy, P.inv2hy) * nbf, nbf - 1.0f));
   return iy * xy_bins + ix;
 }
 
