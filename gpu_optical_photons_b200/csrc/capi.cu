@@ -689,15 +689,20 @@ int run_error(unsigned error) {
   return OPTX_OK;
 }
 
-int engine_check_ctrl(optx_engine* e, WaveCtrl& c, cudaStream_t st) {
-  OPTX_CUDA(cudaMemcpyAsync(&c, e->d_ctrl, sizeof(c), cudaMemcpyDeviceToHost, st));
-  OPTX_CUDA(cudaStreamSynchronize(st));
+// The error a finished run left in its control block.
+int ctrl_error(const WaveCtrl& c) {
   if (c.gs_error & 1u)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "a device genstep is invalid (event index out of range, "
                                            "non-finite coordinate or time, or t1 < t0)");
   if (c.gs_error & 2u)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "device gensteps exceed the engine's max_photons");
   return run_error(c.error);
+}
+
+int engine_check_ctrl(optx_engine* e, WaveCtrl& c, cudaStream_t st) {
+  OPTX_CUDA(cudaMemcpyAsync(&c, e->d_ctrl, sizeof(c), cudaMemcpyDeviceToHost, st));
+  OPTX_CUDA(cudaStreamSynchronize(st));
+  return ctrl_error(c);
 }
 
 }  // namespace
@@ -1414,6 +1419,32 @@ static int engine_upload_records(optx_engine* e, cudaStream_t st) {
   return OPTX_OK;
 }
 
+static int fill_stats(optx_engine* e, const WaveCtrl& c, optx_event_stats* stats) {
+  stats->launches = c.wave;
+  stats->useful_lane_steps = c.useful;
+  stats->issued_lane_steps = c.issued;
+  stats->spills = c.spills;
+  float ms = 0.f;
+  if (e->timed) OPTX_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+  stats->kernels_ms = ms;
+  return OPTX_OK;
+}
+
+// End of the one-shot host-buffer runs: one wait for the run. The tallies and
+// the control block are copied back together (the tally copy first, so that a
+// pageable host_out does not wait twice) and the statistics come from that copy;
+// optx_engine_get_tallies followed by optx_engine_stats would wait three times.
+static int read_back_one_shot(optx_engine* e, uint64_t* host_tallies, optx_event_stats* stats) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  WaveCtrl c{};
+  OPTX_CUDA(cudaMemcpyAsync(host_tallies, e->d_tally, 8ull * e->tdev.len * e->n_tallies,
+                            cudaMemcpyDeviceToHost, nullptr));
+  OPTX_CUDA(cudaMemcpyAsync(&c, e->d_ctrl, sizeof(c), cudaMemcpyDeviceToHost, nullptr));
+  OPTX_CUDA(cudaStreamSynchronize(nullptr));
+  OPTX_TRY(ctrl_error(c));
+  return fill_stats(e, c, stats);
+}
+
 extern "C" {
 
 int optx_engine_set_events(optx_engine* e, const optx_params* events, const optx_faces* faces,
@@ -1588,10 +1619,9 @@ int optx_run_gensteps(optx_engine* e, const optx_params* events, const optx_face
   const auto t0 = std::chrono::steady_clock::now();
   OPTX_TRY(optx_engine_set_gensteps(e, events, faces, n_events, gensteps, n_gensteps, first_id, nullptr));
   OPTX_TRY(optx_engine_run_tally(e, nullptr));
-  OPTX_TRY(optx_engine_get_tallies(e, host_tallies, nullptr));
-  tm.total_ms = ms_since(t0);
   optx_event_stats s{};
-  OPTX_TRY(optx_engine_stats(e, &s, nullptr));
+  OPTX_TRY(read_back_one_shot(e, host_tallies, &s));
+  tm.total_ms = ms_since(t0);
   tm.kernel_ms = s.kernels_ms;
   if (stats) *stats = s;
   if (timing) *timing = tm;
@@ -1734,17 +1764,9 @@ int optx_engine_stats(optx_engine* e, optx_event_stats* stats, void* stream) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (e == nullptr || stats == nullptr)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "engine and stats must not be NULL");
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   WaveCtrl c{};
-  OPTX_TRY(engine_check_ctrl(e, c, st));
-  stats->launches = c.wave;
-  stats->useful_lane_steps = c.useful;
-  stats->issued_lane_steps = c.issued;
-  stats->spills = c.spills;
-  float ms = 0.f;
-  if (e->timed) OPTX_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
-  stats->kernels_ms = ms;
-  return OPTX_OK;
+  OPTX_TRY(engine_check_ctrl(e, c, static_cast<cudaStream_t>(stream)));
+  return fill_stats(e, c, stats);
 }
 
 int optx_run_batch(optx_engine* e, const optx_params* events, const optx_faces* faces,
@@ -1756,10 +1778,9 @@ int optx_run_batch(optx_engine* e, const optx_params* events, const optx_faces* 
   const auto t0 = std::chrono::steady_clock::now();
   OPTX_TRY(optx_engine_set_events(e, events, faces, counts, n_events, first_id, nullptr));
   OPTX_TRY(optx_engine_run_tally(e, nullptr));
-  OPTX_TRY(optx_engine_get_tallies(e, host_tallies, nullptr));
-  tm.total_ms = ms_since(t0);
   optx_event_stats s{};
-  OPTX_TRY(optx_engine_stats(e, &s, nullptr));
+  OPTX_TRY(read_back_one_shot(e, host_tallies, &s));
+  tm.total_ms = ms_since(t0);
   tm.kernel_ms = s.kernels_ms;
   if (stats) *stats = s;
   if (timing) *timing = tm;

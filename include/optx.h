@@ -327,13 +327,15 @@ int optx_engine_get_tallies(optx_engine* e, uint64_t* host_out, void* stream);
 /* Statistics of the last run (synchronises `stream`). */
 int optx_engine_stats(optx_engine* e, optx_event_stats* stats, void* stream);
 /* One-shot batched run with host buffers: H2D of the event table, one graph
- * launch, D2H of the per-event tallies (host_tallies: n_events x tally length). */
+ * launch, D2H of the per-event tallies (host_tallies: n_events x tally length),
+ * with one wait for the run. On an error return host_tallies is unspecified. */
 int optx_run_batch(optx_engine* e, const optx_params* events, const optx_faces* faces,
                    const uint64_t* counts, uint32_t n_events, uint64_t first_id,
                    uint64_t* host_tallies, optx_event_stats* stats, optx_timing* timing);
 
 /* One-shot genstep run with host buffers (extension): set_gensteps, one graph
- * launch, D2H of the per-event tallies (host_tallies: n_events x tally length). */
+ * launch, D2H of the per-event tallies (host_tallies: n_events x tally length),
+ * with one wait for the run. On an error return host_tallies is unspecified. */
 int optx_run_gensteps(optx_engine* e, const optx_params* events, const optx_faces* faces,
                       uint32_t n_events, const optx_genstep* gensteps, uint32_t n_gensteps,
                       uint64_t first_id, uint64_t* host_tallies, optx_event_stats* stats,

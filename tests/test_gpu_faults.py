@@ -45,9 +45,18 @@ def test_watchdog_ends_the_run_and_the_engine_recovers(engine, monkeypatch):
     monkeypatch.delenv("OPTX_TEST_FAULT")
     eng.run_tally()  # the next run resets the control block
     got = eng.tallies()[0]
+    # The one-shot host-buffer calls read the error word in their single wait.
+    monkeypatch.setenv("OPTX_TEST_FAULT", "watchdog")
+    with pytest.raises(OptxError) as e:
+        eng.run_batch([p], [n])
+    assert e.value.code == OPTX_ERR_WATCHDOG
+    monkeypatch.delenv("OPTX_TEST_FAULT")
+    out, st, _ = eng.run_batch([p], [n])
     eng.close()
     _, ref, _ = engine.run_gpu_tally(p, c, n, math="exact")
     assert np.array_equal(got, ref)
+    assert np.array_equal(out[0], ref)
+    assert st["launches"] > 1 and st["useful_lane_steps"] == int(ref[-2] + ref[-1] + ref[1])
 
 
 @pytest.mark.parametrize("bad", [
