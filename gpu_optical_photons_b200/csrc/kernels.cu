@@ -211,8 +211,8 @@ __device__ __forceinline__ uint32_t find_event(const WaveArgs* __restrict__ A, u
 // own entries, k in [ceil(offsets[e] / 2^shift), ceil(offsets[e+1] / 2^shift)),
 // one warp per record (an empty record has none): every entry is written once,
 // with no search per entry. For the 4096-event batch's 519k entries: 7-9 us
-// (CUDA events, warm), 80 us under ncu with cold caches (116 us with a binary
-// search per entry).
+// (CUDA events, warm), against 11-13 us for a thread per entry with a binary
+// search over the offsets.
 __global__ void event_table_kernel(const unsigned long long* __restrict__ offsets, uint32_t n_events,
                                    uint32_t* __restrict__ table, uint32_t shift) {
   const uint32_t lane = threadIdx.x & 31u;
