@@ -48,6 +48,24 @@ def test_genstep_tallies_exact_equal_oracle(engine, oracle, cfg):
         check_tally_consistency(row, TC)
 
 
+def test_genstep_events_with_per_face_surfaces_exact_equal_oracle(engine, oracle):
+    """Gensteps emitting into events whose faces have their own surface model and
+    reflectivity (each photon reads its face parameters from its event's record)."""
+    events, g = _workload(n_events=12, seed=23)
+    rng = np.random.default_rng(23)
+    models = [P.LAMBERTIAN, P.SPECULAR, P.POLISHED, P.BLACK]
+    events = [e.replace(face_surface=[int(models[j]) for j in rng.integers(0, 4, size=5)] + [0],
+                        face_reflectivity=[float(np.float32(x)) for x in rng.uniform(0.8, 0.99, 5)] + [0.0])
+              for e in events]
+    eng = _engine(events, g)
+    eng.set_gensteps(events, g, first_id=61)
+    eng.run_tally()
+    got = eng.tallies()
+    eng.close()
+    ref, _ = oracle.genstep_run(events, g, TC, first_id=61, mode=oracle.PORTABLE)
+    assert np.array_equal(got, ref)
+
+
 def test_genstep_records_exact_equal_oracle(engine, oracle):
     import torch
     events, g = _workload(n_events=8, ppm=30.0)

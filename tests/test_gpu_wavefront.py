@@ -104,6 +104,45 @@ def test_batched_events_large_step_limits_equal_oracle(engine, oracle, max_steps
     assert np.array_equal(got, oracle.batch_tally(arr, offs, c, mode=oracle.PORTABLE))
 
 
+def test_batched_events_with_per_face_surfaces(engine, oracle):
+    """Events with their own surface model and reflectivity on each face: the
+    batched kernel reads a face's reflectivity from the event record by face
+    index. Exact mode equals the oracle event by event; fast mode equals the
+    history kernel (one configuration per launch, face parameters from the
+    kernel argument) event by event."""
+    rng = np.random.default_rng(41)
+    models = [P.LAMBERTIAN, P.SPECULAR, P.POLISHED, P.BLACK]
+    events = []
+    for i in range(24):
+        fs = [int(models[j]) for j in rng.integers(0, 4, size=5)] + [0]
+        fs[i % 5] = P.LAMBERTIAN  # every event keeps at least one painted face
+        fr = [float(np.float32(x)) for x in rng.uniform(0.80, 0.99, size=5)] + [0.0]
+        events.append(P.SimParams(
+            face_surface=fs, face_reflectivity=fr, source=P.VOLUME,
+            abs_length=float(np.float32(rng.uniform(300.0, 3000.0))),
+            scat_length=float("inf") if i % 2 else float(np.float32(rng.uniform(300.0, 1000.0))),
+            n_scint=float(np.float32(rng.uniform(1.5, 1.7)))))
+    counts = rng.integers(1, 12_000, size=len(events)).astype(np.uint64)
+    counts[7] = 0
+    c = P.TallyConfig(100, 50.0, 10)
+    first_id = 300
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64) + np.uint64(first_id)
+    for math_mode in ("exact", "fast"):
+        eng = WavefrontEngine(c, len(events), int(counts.sum()), WaveConfig(math=math_mode))
+        eng.set_events(events, counts, first_id=first_id)
+        eng.run_tally()
+        got = eng.tallies()
+        eng.close()
+        for i, e in enumerate(events):
+            n = int(counts[i])
+            if math_mode == "exact":
+                want = oracle.tally(e, c, n, int(offs[i]), mode=oracle.PORTABLE)
+            else:
+                want = engine.tally_device(e, c, n, first_id=int(offs[i]), math="fast").cpu().numpy()
+            assert np.array_equal(got[i], want.astype(np.uint64)), (math_mode, i, e.face_surface)
+            assert int(got[i, :5].sum()) == n
+
+
 @pytest.mark.parametrize("math_mode", ["exact", "fast"])
 def test_batched_shared_physics_equals_oracle(engine, oracle, math_mode):
     """Events with the same step physics but their own sources, decay times and
