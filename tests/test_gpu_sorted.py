@@ -41,10 +41,23 @@ def test_exact_mode_bitwise_equals_reference_portable_build(engine, golden, name
     assert h["bitwise_identical"] == case["n"], h
 
 
-@pytest.mark.parametrize("cfg", ["config1", "config2", "config3", "config3_ref"])
+MIXED_FACES = P.SimParams(scat_length=600.0, source=P.VOLUME,
+                          face_surface=[P.LAMBERTIAN, P.POLISHED, P.SPECULAR, P.BLACK, P.LAMBERTIAN, 0],
+                          face_reflectivity=[0.9, 0.95, 0.97, 0.5, 0.85, 0.0])
+
+
+def _setup(cfg):
+    if cfg == "config3_ref":
+        return P.config3(black_minus_z=False)[0]
+    if cfg == "mixed_faces":  # every face model, photons moving between all three queues
+        return MIXED_FACES
+    return getattr(P, cfg)()[0]
+
+
+@pytest.mark.parametrize("cfg", ["config1", "config2", "config3", "config3_ref", "mixed_faces"])
 @pytest.mark.parametrize("math_mode", ["fast", "exact", "approx"])
 def test_records_equal_history_kernel(engine, cfg, math_mode):
-    p = P.config3(black_minus_z=False)[0] if cfg == "config3_ref" else getattr(P, cfg)()[0]
+    p = _setup(cfg)
     n = 300_001  # not a multiple of 32
     hist = records_to_numpy(records_device(p, n, first_id=7, math=math_mode))
     for cap, drain in ((0, 0), (4096, 1), (8192, 3000)):
@@ -53,9 +66,9 @@ def test_records_equal_history_kernel(engine, cfg, math_mode):
         assert h["bitwise_identical"] == n, (cap, drain, h)
 
 
-@pytest.mark.parametrize("cfg", ["config1", "config2", "config3"])
+@pytest.mark.parametrize("cfg", ["config1", "config2", "config3", "mixed_faces"])
 def test_tally_equals_history_tally(engine, cfg):
-    p, c = getattr(P, cfg)()
+    p, c = (MIXED_FACES, P.TallyConfig(200, 50.0, 20)) if cfg == "mixed_faces" else getattr(P, cfg)()
     n = 1_000_000
     ref = tally_device(p, c, n).cpu().numpy()
     eng = SortedEngine(1 << 16)

@@ -143,6 +143,38 @@ def test_batched_events_with_per_face_surfaces(engine, oracle):
             assert int(got[i, :5].sum()) == n
 
 
+def test_batched_records_exact_bitwise_equal_oracle(engine, oracle):
+    """Per-photon records of a batch (the batched records variant of the wave
+    kernel, each photon reading its event's record) equal the oracle's records of
+    each event bit for bit in exact mode, in batch order."""
+    import torch
+    events, counts = batched_events(n_events=16, seed=43, median=3000, n_min=1, n_max=15000)
+    events[5] = events[5].replace(face_surface=[P.SPECULAR, P.BLACK, P.LAMBERTIAN, P.POLISHED, P.LAMBERTIAN, 0],
+                                  face_reflectivity=[0.97, 0.5, 0.9, 0.8, 0.93, 0.0],
+                                  scat_length=450.0, source=P.VOLUME)
+    counts[9] = 0
+    n = int(counts.sum())
+    first_id = 4242
+    eng = WavefrontEngine(P.TallyConfig(100, 50.0, 10), len(events), n, WaveConfig(math="exact"))
+    try:
+        eng.set_events(events, counts, first_id=first_id)
+        d = engine.device_records(n)
+        eng.run_records(d)
+        torch.cuda.synchronize()
+        rec = engine.records_to_numpy(d)
+    finally:
+        eng.close()
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    for i, e in enumerate(events):
+        lo, hi = int(offs[i]), int(offs[i + 1])
+        if hi == lo:
+            continue
+        want = oracle.records(e, hi - lo, first_id + lo, mode=oracle.PORTABLE)
+        got = {k: rec[k][lo:hi] for k in rec}
+        h = compare_histories(got, want)
+        assert h["bitwise_identical"] == hi - lo, (i, h)
+
+
 @pytest.mark.parametrize("math_mode", ["exact", "fast"])
 def test_batched_shared_physics_equals_oracle(engine, oracle, math_mode):
     """Events with the same step physics but their own sources, decay times and
