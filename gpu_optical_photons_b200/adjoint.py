@@ -31,15 +31,23 @@ import numpy as np
 import torch
 
 from . import _lib
-from .params import SimParams, TallyConfig
+from .params import LAMBERTIAN, SPECULAR, SimParams, TallyConfig
 from .wavefront import WaveConfig, WavefrontEngine
 
 THETA_NAMES = ("abs_length", "scat_length", "reflectivity", "tau")
 
 
 def with_theta(p: SimParams, theta) -> SimParams:
+    """p at theta = (abs_length, scat_length, R, tau). R is the reflectivity of
+    the painted (specular and Lambertian) faces: with per-face surfaces it is
+    written to each painted face, and faces of other models keep their values."""
     t = [float(np.float32(v)) for v in theta]
-    return p.replace(abs_length=t[0], scat_length=t[1], reflectivity=t[2], tau=t[3])
+    kw = dict(abs_length=t[0], scat_length=t[1], reflectivity=t[2], tau=t[3])
+    if p.face_reflectivity is not None:
+        surf = p.face_surface or [p.surface] * 6
+        kw["face_reflectivity"] = [t[2] if i < 5 and int(surf[i]) in (SPECULAR, LAMBERTIAN) else float(r)
+                                   for i, r in enumerate(p.face_reflectivity)]
+    return p.replace(**kw)
 
 
 class ResponseModel:

@@ -1688,15 +1688,26 @@ int adjoint_setup(optx_engine* e, double inv[7], uint32_t& mask) {
   if (e->n_tallies != 1)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "the adjoint runs on a single-configuration batch");
   const DevParams& P = e->h_params[0];
-  const double la = P.abs_length, ls = P.scat_length, R = P.refl0, tau = P.tau;
+  // R is the reflectivity of the painted (specular / Lambertian) faces: the score
+  // of a reflection there is 1 / R, so with per-face surfaces every painted face
+  // must have that one reflectivity (faces of other models carry none).
+  const float refl[5] = {P.refl0, P.refl1, P.refl2, P.refl3, P.refl4};
+  bool painted = false;
+  float Rf = 0.0f;
+  for (int f = 0; f < 5; ++f) {
+    const uint32_t m = (P.surf_bits >> (2 * f)) & 3u;
+    if (m != kSpecular && m != kLambertian) continue;
+    if (painted && refl[f] != Rf)
+      return fail(OPTX_ERR_INVALID_ARGUMENT,
+                  "the adjoint's reflectivity parameter is one value: the painted faces must share one "
+                  "reflectivity");
+    Rf = refl[f];
+    painted = true;
+  }
+  const double la = P.abs_length, ls = P.scat_length, R = Rf, tau = P.tau;
   mask = 0;
   if (std::isfinite(la)) mask |= 1u;
   if (std::isfinite(ls)) mask |= 2u;
-  bool painted = false;
-  for (int f = 0; f < 5; ++f) {
-    const uint32_t m = (P.surf_bits >> (2 * f)) & 3u;
-    painted = painted || m == kSpecular || m == kLambertian;
-  }
   if (painted && R > 0.0) mask |= 4u;
   if (tau > 0.0) mask |= 8u;
   inv[0] = 1.0 / la;

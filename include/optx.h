@@ -300,7 +300,10 @@ int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* s
  * scat_length, reflectivity, tau):
  *   S_La = path / La^2,  S_Ls = path / Ls^2 - n_scatter / Ls,
  *   S_R = (reflections at painted faces) / R,  S_tau = t_emit / tau^2 - 1 / tau
- * (terms of a disabled process are 0). With w_bin = dLoss/dh (h = the run's
+ * (terms of a disabled process are 0). R is the reflectivity of the painted
+ * (specular and Lambertian) faces: with per-face surfaces (optx_faces) they must
+ * all have the same reflectivity, else OPTX_ERR_INVALID_ARGUMENT; faces of other
+ * models may carry any value. With w_bin = dLoss/dh (h = the run's
  * arrival-time histogram, time_bins + 1 entries) and w_det = dLoss/dD / n
  * (D = detected fraction), grad = dLoss/dtheta. dev_w_bin, dev_grad (4
  * doubles, overwritten): device pointers. Asynchronous on `stream`; a run that

@@ -222,6 +222,54 @@ def test_score_moments_rejects_bad_arguments(engine):
         eng.close()
 
 
+def test_reflectivity_parameter_with_per_face_surfaces(engine):
+    """R is the reflectivity of the painted faces. (1) The same Lambertian box
+    given as per-face lists replays the plain configuration's gradient exactly;
+    (2) a black face's own reflectivity (which no photon uses) does not change
+    the gradient; (3) painted faces with different reflectivities have no single
+    R: the replay and the score moments are refused. A reflectivity taken from
+    the wrong face would scale the R score by 0.95 / 0.2 or 0.95 / 0.5."""
+    import ctypes
+    from gpu_optical_photons_b200 import _lib
+    from gpu_optical_photons_b200.wavefront import WavefrontEngine
+    n = 100_000
+    lam = P.SimParams(surface=P.LAMBERTIAN, reflectivity=0.95, n_det=1.5, source=P.VOLUME,
+                      abs_length=2000.0, scat_length=500.0, tau=4.0)
+    w = torch.as_tensor(np.random.default_rng(3).normal(size=TC.time_bins + 1))
+
+    def grad(base):
+        m = ResponseModel(base, n, TC, first_id=9, config=WaveConfig(math="exact"))
+        try:
+            return m.replay(THETA0, w, 0.3)
+        finally:
+            m.close()
+
+    # The same photons and scores; the FP64 sums are atomics, so equal up to the
+    # order of their additions.
+    same = dict(rtol=1e-12, atol=0.0)
+    plain = grad(lam)
+    listed = grad(lam.replace(face_surface=[P.LAMBERTIAN] * 5 + [0], face_reflectivity=[0.5] * 6))
+    assert np.allclose(listed, plain, **same), (listed, plain)  # theta's R on every painted face
+    black = [P.BLACK] + [P.LAMBERTIAN] * 4 + [0]
+    g1 = grad(lam.replace(face_surface=black, face_reflectivity=[0.2] + [0.95] * 5))
+    g2 = grad(lam.replace(face_surface=black, face_reflectivity=[0.9] + [0.95] * 5))
+    assert np.allclose(g1, g2, **same) and g1[2] != 0.0, (g1, g2)
+    mixed = lam.replace(face_surface=[P.LAMBERTIAN] * 5 + [0], face_reflectivity=[0.9] + [0.95] * 5)
+    eng = WavefrontEngine(TC, 1, 1000)
+    try:
+        eng.set_events([mixed], [1000])
+        buf = torch.zeros(4, dtype=torch.float64, device="cuda")
+        wb = torch.zeros(TC.time_bins + 1, dtype=torch.float64, device="cuda")
+        with pytest.raises(_lib.InvalidArgument, match="painted faces must share one reflectivity"):
+            _lib.call("optx_engine_run_adjoint", eng._h, ctypes.c_void_p(wb.data_ptr()), 0.0,
+                      ctypes.c_void_p(buf.data_ptr()), None)
+        mom = torch.zeros((TC.time_bins + 1) * 5, dtype=torch.float64, device="cuda")
+        with pytest.raises(_lib.InvalidArgument, match="painted faces must share one reflectivity"):
+            _lib.call("optx_engine_run_score_moments", eng._h, ctypes.c_void_p(mom.data_ptr()), None)
+    finally:
+        eng.close()
+
+
 def test_calibration_command_line(engine, capsys):
     import json
     from gpu_optical_photons_b200.adjoint import main
