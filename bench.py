@@ -56,6 +56,17 @@ def workload_name(n_events: int) -> str:
             "[1e2,1e6]), Lambertian cube, per-event tallies")
 
 
+def workload_config(events, counts) -> dict:
+    """The `config` of both arms' lines: the workload alone, identical in both
+    (what each arm ran per step and its timing details are keys of their own).
+    L2: the optx arm writes 256 MB (> the 126 MB L2) between timed steps,
+    outside its CUDA events; the reference arm is CPU code."""
+    return {"workload": workload_name(len(events)), "events": len(events),
+            "photons_per_step": int(np.asarray(counts).sum()),
+            "l2": "optx arm: flushed between timed steps (256 MB write, outside the CUDA events); "
+                  "reference arm: CPU code (no device cache involved)"}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,7 +208,7 @@ def cpu_reference_leg(events, counts, tc, max_events: int, threads: int = 0, fir
             rows.append(t)
     dt = time.perf_counter() - t0
     cores = (O.ref(0).ref_max_threads() if kind == "reference" else os.cpu_count()) if threads == 0 else threads
-    return ({"value": steps / dt, "unit": UNIT, "cores": int(cores), "kind": kind,
+    return ({"value": steps / dt, "unit": UNIT, "cores": int(cores), "kind": kind, "photon_steps": steps,
              "sample": f"events {first}..{max_events - 1} of {len(counts)} ({photons} photons, {steps} photon-steps), "
                        f"run_cpu_tally per event, {dt:.1f} s"}, steps / dt,
             np.stack(rows) if keep else None)
@@ -489,10 +500,10 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median(secs)) * 1e3,
             "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded event generator)",
-            "config": {"workload": workload_name(len(events)),
-                       "events": len(events), "photons_per_step": int(counts.sum()),
-                       "per_step": "the whole batch: run_cpu_tally per event (all host threads)",
-                       "warmup_steps": f"{warm}-event slice"},
+            "config": workload_config(events, counts),
+            "per_step": "the whole batch: run_cpu_tally per event (all host threads)",
+            "warmup_steps": f"{warm}-event slice",
+            "photon_steps_per_step": base["photon_steps"],
             "cpu_baseline": {**base, "value": value,
                              "sample": "the whole batch per step; " + base["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -839,18 +850,17 @@ def run_optx(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded event generator)",
-        "config": {"workload": workload_name(len(events)),
-                   "events": len(events), "photons_per_step": n_photons,
-                   "photon_steps_per_step": steps_per_run, "photons_per_s": world * n_photons / (ms_step * 1e-3),
-                   "l2": "flushed between timed steps (256 MB write, outside the CUDA events)",
-                   "autotune": tuned,
-                   "engine": {"block_size": cfg.block_size, "threshold": cfg.threshold,
-                              "wave_quota": cfg.wave_quota,
-                              "blocks_per_sm": cfg.blocks_per_sm,
-                              "cadence": cfg.cadence, "chunk": cfg.chunk or 256,
-                              "tail_steps": cfg.tail_steps or 4096,
-                              "graph": cfg.use_graph, "math": cfg.math},
-                   "parallelism": f"dp{world} (independent event batches per GPU)"},
+        "config": workload_config(events, counts),
+        "photon_steps_per_step": steps_per_run,
+        "photons_per_s": world * n_photons / (ms_step * 1e-3),
+        "parallelism": f"dp{world} (independent event batches per GPU)",
+        "autotune": tuned,
+        "engine": {"block_size": cfg.launch_block_size, "threshold": cfg.threshold,
+                   "wave_quota": cfg.wave_quota,
+                   "blocks_per_sm": cfg.blocks_per_sm,
+                   "cadence": cfg.cadence, "chunk": cfg.chunk or 256,
+                   "tail_steps": cfg.tail_steps or 4096,
+                   "graph": cfg.use_graph, "math": cfg.math},
         "e2e": {"value": world * steps_per_run / (e2e_step * 1e-3), "unit": UNIT,
                 "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                 "ms_per_step": e2e_step, "call": "optx_run_batch (pinned host buffers)"},

@@ -32,10 +32,14 @@ class WaveConfig:
     max_gensteps: int = 0       # capacity for set_gensteps (0 = no gensteps)
     tail_steps: int = 0         # steps in a wave before a photon may move to the next (0 = 4096)
 
+    @property
+    def launch_block_size(self) -> int:
+        """Threads per block of the launches: the 72-register budget (7 blocks
+        per SM) runs 128-thread blocks when the default 256 is given."""
+        return 128 if self.blocks_per_sm == 7 and self.block_size == 256 else self.block_size
+
     def to_c(self) -> _lib.CWaveConfig:
-        # the 72-register budget runs 128-thread blocks
-        bs = 128 if self.blocks_per_sm == 7 and self.block_size == 256 else self.block_size
-        return _lib.CWaveConfig(bs, self.blocks_per_sm, self.threshold, self.cadence,
+        return _lib.CWaveConfig(self.launch_block_size, self.blocks_per_sm, self.threshold, self.cadence,
                                 self.wave_quota, 1 if self.use_graph else -1, _lib.MATH[self.math],
                                 self.chunk, self.max_gensteps, self.tail_steps, 0)
 
