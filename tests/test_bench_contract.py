@@ -32,6 +32,15 @@ def test_reference_arm_prints_one_contract_line(oracle):
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
+    # Both arms name the same workload: the optx arm's `config` is built by the
+    # same function from the same events (its line carries run details as
+    # keys of their own), so the two configs are equal.
+    sys.path.insert(0, ROOT)
+    import bench
+    from gpu_optical_photons_b200.wavefront import batched_events
+    events, counts = batched_events(n_events=16)
+    assert d["config"] == bench.workload_config(events, counts)
+    assert d["photon_steps_per_step"] == cb["photon_steps"] > 0
 
 
 def test_reference_arm_other_ranks_exit_quietly():
