@@ -297,10 +297,21 @@ def batch_fingerprint(events, counts, first_id: int, tally: TallyConfig) -> str:
 
 
 def save_checkpoint(path: str, fingerprint: str, next_index: int, tallies) -> None:
-    """Writes a checkpoint (.npz): the batch fingerprint, the next relative photon
-    index and the per-event tallies so far."""
-    np.savez(path, fingerprint=np.array(fingerprint), next_index=np.uint64(next_index),
-             tallies=np.ascontiguousarray(tallies, dtype=np.uint64))
+    """Writes a checkpoint (.npz format): the batch fingerprint, the next relative
+    photon index and the per-event tallies so far. The file is written under
+    exactly `path` (no extension is added, so the next run finds it there) and
+    replaces the previous checkpoint in one rename: a run killed while writing
+    leaves the previous checkpoint intact."""
+    import os
+    tmp = f"{path}.tmp{os.getpid()}"
+    try:
+        with open(tmp, "wb") as f:  # a file object: np.savez appends no ".npz"
+            np.savez(f, fingerprint=np.array(fingerprint), next_index=np.uint64(next_index),
+                     tallies=np.ascontiguousarray(tallies, dtype=np.uint64))
+        os.replace(tmp, path)
+    finally:
+        if os.path.exists(tmp):
+            os.remove(tmp)
 
 
 def load_checkpoint(path: str, fingerprint: str):

@@ -39,3 +39,18 @@ def test_fingerprint_tracks_the_batch(tmp_path):
     save_checkpoint(path, fp, 10, np.zeros((12, tc.length), np.uint64))
     with pytest.raises(ValueError, match="another batch"):
         load_checkpoint(path, others[0])
+
+
+def test_checkpoint_written_under_the_given_name(tmp_path):
+    """A path without the .npz extension is written as given (the next run looks
+    for exactly that file), and a second save replaces the first in place with
+    no temporary file left behind."""
+    events, counts = batched_events(n_events=4, seed=3, median=500)
+    tc = P.TallyConfig(10, 50.0, 2)
+    fp = batch_fingerprint(events, counts, 0, tc)
+    path = str(tmp_path / "run.ckpt")
+    save_checkpoint(path, fp, 5, np.ones((4, tc.length), np.uint64))
+    save_checkpoint(path, fp, 9, np.full((4, tc.length), 3, np.uint64))
+    assert sorted(p.name for p in tmp_path.iterdir()) == ["run.ckpt"]
+    nxt, t = load_checkpoint(path, fp)
+    assert nxt == 9 and np.array_equal(t, np.full((4, tc.length), 3, np.uint64))
