@@ -58,6 +58,10 @@ def main(argv=None):
     ap.add_argument("--seed", type=int)
     ap.add_argument("--max_steps", type=int)
     a = ap.parse_args(argv)
+    if a.repeat < 1:
+        ap.error("--repeat must be >= 1")
+    if a.engine == "gensteps" and a.mode == "records":
+        ap.error("--engine gensteps runs in tally mode only (per-event tallies)")
 
     import torch
     import gpu_optical_photons_b200 as g
@@ -159,14 +163,27 @@ def main(argv=None):
                          blocks_per_sm=a.bps, chunk=a.chunk, use_graph=not a.host_loop, math=a.math)
         eng = WavefrontEngine(c, 1, n, cfg)
         eng.set_events([p], [n])
+        rec = g.device_records(n) if a.mode == "records" else None
         for _ in range(a.repeat):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            eng.run_tally()
+            if rec is None:
+                eng.run_tally()
+            else:
+                eng.run_records(rec)
             torch.cuda.synchronize()
             times.append((time.perf_counter() - t0) * 1e3)
-        flat = eng.tallies()[0]
         out["stats"] = eng.stats()
+        if rec is None:
+            flat = eng.tallies()[0]
+        else:
+            r = g.records_to_numpy(rec)
+            flat = None
+            out["steps"] = int(r.steps().sum())
+            if a.out:
+                from . import io
+                meta = io.params_to_json(p, io.RunOptions("gpu", "records", n, 1, a.block, c))
+                io.write_records(a.out, r, meta)
         eng.close()
     if flat is not None:
         t = g.Tally.from_flat(flat, c)

@@ -202,3 +202,13 @@ def test_cli_engines_print_a_consistent_line(engine, capsys, tmp_path, argv):
     if not gs:
         t = IO.read_tally(str(out_dir))
         assert int(np.asarray(t.fate_counts).sum()) == n
+
+
+@pytest.mark.parametrize("argv", [["--engine", "gensteps", "--mode", "records"], ["--repeat", "0"]])
+def test_cli_rejects_unsupported_options(argv, capsys):
+    """Options the runner cannot honour end with a usage error before any GPU work."""
+    from gpu_optical_photons_b200 import cli
+    with pytest.raises(SystemExit) as ei:
+        cli.main(argv)
+    assert ei.value.code == 2
+    assert "error" in capsys.readouterr().err
