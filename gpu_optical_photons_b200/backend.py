@@ -35,15 +35,27 @@ class Records(dict):
     FIELDS = ("fate", "n_boundary", "n_scatter", "t", "x", "y", "z", "path")
     BYTES_PER_PHOTON = 29
 
+    DTYPES = {"fate": np.uint8, "n_boundary": np.uint32, "n_scatter": np.uint32, "t": np.float32,
+              "x": np.float32, "y": np.float32, "z": np.float32, "path": np.float32}
+
     @staticmethod
     def empty(n: int) -> "Records":
         r = Records()
-        r["fate"] = np.zeros(n, np.uint8)
-        r["n_boundary"] = np.zeros(n, np.uint32)
-        r["n_scatter"] = np.zeros(n, np.uint32)
-        for k in ("t", "x", "y", "z", "path"):
-            r[k] = np.zeros(n, np.float32)
+        for k in Records.FIELDS:
+            r[k] = np.zeros(n, Records.DTYPES[k])
         return r
+
+    def resize(self, n: int) -> "Records":
+        """Makes every field a writable, C-contiguous array of n entries of its
+        type, replacing the fields that are not (the reference's callee resizes
+        the caller's vectors, cpu_backend.cpp:40-49): the C ABI writes n entries
+        through each field's pointer."""
+        for k in self.FIELDS:
+            v = self.get(k)
+            if not (isinstance(v, np.ndarray) and v.dtype == self.DTYPES[k] and v.ndim == 1
+                    and v.shape[0] == n and v.flags.c_contiguous and v.flags.writeable):
+                self[k] = np.zeros(n, self.DTYPES[k])
+        return self
 
     def c_struct(self) -> _lib.CRecords:
         return _lib.CRecords(*[self[k].ctypes.data for k in self.FIELDS])
@@ -100,7 +112,7 @@ def _math(math) -> int:
 def run_gpu_records(p: SimParams, n: int, block_size: int = 256, first_id: int = 0,
                     chunk: int = 1 << 24, math="fast", out: Records | None = None):
     """Records of photons first_id .. first_id + n - 1 (gpu_backend.cu:119-156). Returns (Records, timing)."""
-    out = Records.empty(n) if out is None else out
+    out = Records.empty(n) if out is None else out.resize(n)
     cp, cf = _lib.params_args(p)
     cr = out.c_struct()
     tm = _lib.CTiming()

@@ -212,3 +212,27 @@ def test_cli_rejects_unsupported_options(argv, capsys):
         cli.main(argv)
     assert ei.value.code == 2
     assert "error" in capsys.readouterr().err
+
+
+def test_records_resize_replaces_unusable_fields():
+    """run_gpu_records writes n entries through each field's pointer, so a
+    caller's Records is resized first (the reference resizes the caller's
+    vectors): short, long, strided, read-only or wrongly typed fields are
+    replaced; fields already fit for n entries are kept as they are."""
+    from gpu_optical_photons_b200.backend import Records
+    n = 10
+    r = Records.empty(n)
+    keep = r["t"]
+    r["fate"] = np.zeros(3, np.uint8)                       # too short
+    r["n_boundary"] = np.zeros(20, np.uint32)               # too long
+    r["x"] = np.zeros(2 * n, np.float32)[::2]               # strided
+    ro = np.zeros(n, np.float32)
+    ro.flags.writeable = False
+    r["y"] = ro                                              # read-only
+    r["z"] = np.zeros(n, np.float64)                         # wrong type
+    del r["path"]                                            # missing
+    r.resize(n)
+    assert r["t"] is keep
+    for k in Records.FIELDS:
+        v = r[k]
+        assert v.shape == (n,) and v.dtype == Records.DTYPES[k] and v.flags.c_contiguous and v.flags.writeable
