@@ -204,6 +204,22 @@ def test_cli_engines_print_a_consistent_line(engine, capsys, tmp_path, argv):
         assert int(np.asarray(t.fate_counts).sum()) == n
 
 
+@pytest.mark.gpu
+def test_cli_wave_records_equal_history_records(engine, capsys, tmp_path):
+    """--engine wave --mode records writes the engine's per-photon records, which
+    equal the history kernel's bit for bit (exact math)."""
+    import json
+    from gpu_optical_photons_b200 import cli
+    base = ["--config", "config2", "--mode", "records", "--n", "50000", "--math", "exact", "--repeat", "1"]
+    cli.main(base + ["--engine", "wave", "--out", str(tmp_path / "w")])
+    cli.main(base + ["--engine", "history", "--out", str(tmp_path / "h")])
+    lines = [json.loads(l) for l in capsys.readouterr().out.strip().splitlines()]
+    assert lines[0]["steps"] == lines[1]["steps"] > 0
+    w, h = IO.read_records(str(tmp_path / "w")), IO.read_records(str(tmp_path / "h"))
+    for k in ("fate", "n_boundary", "n_scatter", "t", "x", "y", "z", "path"):
+        assert np.array_equal(np.asarray(w[k]).view(np.uint8), np.asarray(h[k]).view(np.uint8)), k
+
+
 @pytest.mark.parametrize("argv", [["--engine", "gensteps", "--mode", "records"], ["--repeat", "0"]])
 def test_cli_rejects_unsupported_options(argv, capsys):
     """Options the runner cannot honour end with a usage error before any GPU work."""
