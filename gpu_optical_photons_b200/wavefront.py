@@ -58,6 +58,15 @@ class EventTable:
         return self.n
 
 
+def _counts_c(counts, n_events: int) -> np.ndarray:
+    """Photon counts as the C ABI reads them: one uint64 per event (the call
+    reads n_events entries through the pointer)."""
+    cnt = np.ascontiguousarray(counts, dtype=np.uint64)
+    if cnt.ndim != 1 or cnt.shape[0] != n_events:
+        raise ValueError(f"counts must hold one photon count per event ({n_events}), got shape {cnt.shape}")
+    return cnt
+
+
 def _events_c(events):
     if isinstance(events, EventTable):
         return events.arr, events.faces
@@ -105,7 +114,7 @@ class WavefrontEngine:
     def set_events(self, events, counts, first_id: int = 0, stream=0):
         """Uploads a batch; `events` is a list of SimParams (or CSimParams)."""
         arr, faces = _events_c(events)
-        cnt = np.ascontiguousarray(counts, dtype=np.uint64)
+        cnt = _counts_c(counts, len(arr))
         self._keep = (arr, faces, cnt)
         _lib.call("optx_engine_set_events", self._h, ctypes.cast(arr, ctypes.c_void_p),
                   ctypes.cast(faces, ctypes.c_void_p) if faces is not None else None,
@@ -204,7 +213,7 @@ class WavefrontEngine:
     def run_batch(self, events, counts, first_id: int = 0):
         """One-shot host-buffer run: H2D table, graph launch, D2H tallies."""
         arr, faces = _events_c(events)
-        cnt = np.ascontiguousarray(counts, dtype=np.uint64)
+        cnt = _counts_c(counts, len(arr))
         out = np.zeros((len(events), self.tally_config.length), np.uint64)
         st = _lib.CEventStats()
         tm = _lib.CTiming()

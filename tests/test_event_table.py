@@ -23,3 +23,15 @@ def test_event_table_with_per_face_surfaces():
     arr, faces = _events_c(events)
     assert faces is not None and bytes(tab.faces) == bytes(faces) and bytes(tab.arr) == bytes(arr)
     assert ctypes.sizeof(tab.faces) == 3 * 48
+
+
+def test_counts_must_match_the_events():
+    """The engine calls read one photon count per event through a raw pointer:
+    counts of another length (or shape) are refused before the call."""
+    import numpy as np
+    import pytest
+    from gpu_optical_photons_b200.wavefront import _counts_c
+    assert _counts_c([3, 4, 5], 3).dtype == np.uint64
+    for bad in ([3, 4], [3, 4, 5, 6], [[3, 4, 5]]):
+        with pytest.raises(ValueError, match="one photon count per event"):
+            _counts_c(bad, 3)
