@@ -80,7 +80,9 @@ class ResponseModel:
         """FP64 sum over detected photons of (w_bin[bin] + w_det) * score."""
         self._upload(theta)
         w = w_bin.detach().to(device="cuda", dtype=torch.float64).contiguous()
-        assert w.numel() == self.tally.time_bins + 1
+        if w.numel() != self.tally.time_bins + 1:  # the kernel reads time_bins + 1 weights
+            raise ValueError(f"w_bin must hold time_bins + 1 = {self.tally.time_bins + 1} weights, "
+                             f"got {w.numel()}")
         grad = torch.zeros(4, dtype=torch.float64, device="cuda")
         stream = torch.cuda.current_stream().cuda_stream
         _lib.call("optx_engine_run_adjoint", self.engine._h, ctypes.c_void_p(w.data_ptr()),
