@@ -222,6 +222,20 @@ def test_score_moments_rejects_bad_arguments(engine):
         eng.close()
 
 
+def test_replay_rejects_weights_of_another_length(engine):
+    """The replay kernel reads time_bins + 1 bin weights: a shorter or longer
+    vector is refused before the launch, and the model stays usable."""
+    m = ResponseModel(BASE, 1000, TC)
+    try:
+        for k in (TC.time_bins, TC.time_bins + 2):
+            with pytest.raises(ValueError, match="time_bins \\+ 1"):
+                m.replay(THETA0, torch.ones(k, dtype=torch.float64), 0.0)
+        g = m.replay(THETA0, torch.ones(TC.time_bins + 1, dtype=torch.float64), 0.0)
+        assert g.shape == (4,) and np.all(np.isfinite(g))
+    finally:
+        m.close()
+
+
 def test_reflectivity_parameter_with_per_face_surfaces(engine):
     """R is the reflectivity of the painted faces. (1) The same Lambertian box
     given as per-face lists replays the plain configuration's gradient exactly;
