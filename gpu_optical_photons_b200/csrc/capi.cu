@@ -1727,6 +1727,8 @@ int optx_engine_run_adjoint(optx_engine* e, const double* dev_w_bin, double w_de
   std::lock_guard<std::mutex> lk(g_mu);
   if (e == nullptr || dev_w_bin == nullptr || dev_grad == nullptr)
     return fail(OPTX_ERR_INVALID_ARGUMENT, "engine, dev_w_bin and dev_grad must not be NULL");
+  if ((reinterpret_cast<uintptr_t>(dev_w_bin) & 7u) != 0u)  // the kernel reads it as doubles
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "dev_w_bin must be 8-byte aligned");
   double inv[7];
   uint32_t mask = 0;
   OPTX_TRY(adjoint_setup(e, inv, mask));

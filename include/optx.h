@@ -305,7 +305,8 @@ int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* s
  * all have the same reflectivity, else OPTX_ERR_INVALID_ARGUMENT; faces of other
  * models may carry any value. With w_bin = dLoss/dh (h = the run's
  * arrival-time histogram, time_bins + 1 entries) and w_det = dLoss/dD / n
- * (D = detected fraction), grad = dLoss/dtheta. dev_w_bin, dev_grad (4
+ * (D = detected fraction), grad = dLoss/dtheta. dev_w_bin (time_bins + 1
+ * doubles, 8-byte aligned, else OPTX_ERR_INVALID_ARGUMENT), dev_grad (4
  * doubles, overwritten): device pointers. Asynchronous on `stream`; a run that
  * ends on the watchdog or a full state queue is reported by the next
  * optx_engine_stats / optx_engine_get_tallies on the engine. */

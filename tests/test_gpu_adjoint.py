@@ -210,6 +210,10 @@ def test_score_moments_rejects_bad_arguments(engine):
         with pytest.raises(_lib.OptxError):  # not 8-byte aligned
             _lib.call("optx_engine_run_score_moments", m.engine._h,
                       ctypes.c_void_p(buf.data_ptr() + 4), None)
+        grad = torch.zeros(4, dtype=torch.float64, device="cuda")
+        with pytest.raises(_lib.OptxError, match="8-byte aligned"):  # bin weights not 8-byte aligned
+            _lib.call("optx_engine_run_adjoint", m.engine._h, ctypes.c_void_p(buf.data_ptr() + 4), 0.0,
+                      ctypes.c_void_p(grad.data_ptr()), None)
     finally:
         m.close()
     eng = WavefrontEngine(TC, 2, 2000)
