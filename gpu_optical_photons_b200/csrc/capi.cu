@@ -278,6 +278,26 @@ int check_records(const optx_records* r) {
   return OPTX_OK;
 }
 
+// Device record arrays and tallies are written by kernels: n_boundary, n_scatter
+// and the float fields with 4-byte stores, tallies with 64-bit atomics. A
+// misaligned pointer would fault the GPU inside the kernel, so it is refused here.
+int check_dev_records(const optx_records* r) {
+  OPTX_TRY(check_records(r));
+  const void* words[7] = {r->n_boundary, r->n_scatter, r->t, r->x, r->y, r->z, r->path};
+  for (const void* w : words)
+    if ((reinterpret_cast<uintptr_t>(w) & 3u) != 0u)
+      return fail(OPTX_ERR_INVALID_ARGUMENT,
+                  "device records: n_boundary, n_scatter, t, x, y, z and path must be 4-byte aligned");
+  return OPTX_OK;
+}
+
+int check_dev_tally(const uint64_t* t) {
+  if (t == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "dev_tally must not be NULL");
+  if ((reinterpret_cast<uintptr_t>(t) & 7u) != 0u)
+    return fail(OPTX_ERR_INVALID_ARGUMENT, "dev_tally must be 8-byte aligned (64-bit atomics)");
+  return OPTX_OK;
+}
+
 DevRecords to_dev(const optx_records* r) {
   return {r->fate, r->n_boundary, r->n_scatter, r->t, r->x, r->y, r->z, r->path};
 }
@@ -1206,7 +1226,7 @@ int optx_records_device(const optx_params* p, const optx_faces* faces, uint64_t 
   OPTX_TRY(check_params(p, faces));
   OPTX_TRY(check_block(block_size));
   OPTX_TRY(check_math(math));
-  if (n > 0) OPTX_TRY(check_records(dev_out));
+  if (n > 0) OPTX_TRY(check_dev_records(dev_out));
   OPTX_TRY(ensure_device());
   const DevParams P = make_dev_params(*p, faces);
   const DevRecords d = to_dev(dev_out);
@@ -1237,7 +1257,7 @@ int optx_tally_device(const optx_params* p, const optx_faces* faces, const optx_
   OPTX_TRY(check_math(math));
   TallyDev td{};
   OPTX_TRY(make_tally_dev(c, td));
-  if (dev_tally == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "dev_tally must not be NULL");
+  OPTX_TRY(check_dev_tally(dev_tally));
   OPTX_TRY(ensure_device());
   const size_t smem = static_cast<size_t>(td.len - 7u) * 4u;
   int dev = 0, max_smem = 0;
@@ -1673,7 +1693,7 @@ int optx_engine_set_tallies(optx_engine* e, const uint64_t* host_tallies, void* 
 int optx_engine_run_records(optx_engine* e, const optx_records* dev_out, void* stream) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (e == nullptr) return fail(OPTX_ERR_INVALID_ARGUMENT, "engine must not be NULL");
-  OPTX_TRY(check_records(dev_out));
+  OPTX_TRY(check_dev_records(dev_out));
   const DevRecords d = to_dev(dev_out);
   return engine_run(e, kModeRecords, &d, nullptr, 0.0, nullptr, 0u,
                     static_cast<cudaStream_t>(stream));
@@ -2041,7 +2061,8 @@ int optx_sorted_run(optx_sorted* s, const optx_params* p, const optx_faces* face
     return fail(OPTX_ERR_INVALID_ARGUMENT, "give dev_tally, dev_records or both");
   TallyDev td{};
   if (dev_tally != nullptr) OPTX_TRY(make_tally_dev(c, td));
-  if (dev_records != nullptr) OPTX_TRY(check_records(dev_records));
+  if (dev_tally != nullptr) OPTX_TRY(check_dev_tally(dev_tally));
+  if (dev_records != nullptr) OPTX_TRY(check_dev_records(dev_records));
   if (n >= (1ull << 32)) return fail(OPTX_ERR_INVALID_ARGUMENT, "at most 2^32 - 1 photons per run");
   std::lock_guard<std::mutex> lk(s->mu);
   if (n == 0) return OPTX_OK;

@@ -171,6 +171,10 @@ int optx_run_records_event(const optx_params* p, const optx_faces* faces, uint64
                            optx_timing* timing);
 
 /* ---- device-resident calls (caller device buffers, async on `stream`) --- */
+/* Device buffers given to these calls and to optx_engine_run_records /
+ * optx_sorted_run are written by kernels: the record arrays n_boundary,
+ * n_scatter, t, x, y, z, path must be 4-byte aligned and tallies 8-byte
+ * aligned, else OPTX_ERR_INVALID_ARGUMENT before any launch. */
 /* History records kernel into device arrays of n entries. */
 int optx_records_device(const optx_params* p, const optx_faces* faces, uint64_t n,
                         uint64_t first_id, const optx_records* dev_out, int block_size, int math,

@@ -102,6 +102,25 @@ def test_sorted_run_rejects_invalid_arguments_before_any_device_call(lib):
     assert lib.optx_sorted_destroy(None) == 0
 
 
+def test_misaligned_device_buffers_are_refused_before_any_device_call(lib):
+    """Kernels write device records with 4-byte stores and tallies with 64-bit
+    atomics: misaligned pointers are refused on the host (a launch would fault the
+    GPU). The addresses are never dereferenced: every call fails its checks."""
+    cp = P.SimParams().to_c()
+    base = 1 << 20
+    good = [base + 4096 * i for i in range(8)]
+    for field in range(1, 8):  # n_boundary, n_scatter, t, x, y, z, path
+        ptrs = list(good)
+        ptrs[field] += 2
+        rec = _lib.CRecords(*ptrs)
+        with pytest.raises(ValueError, match="4-byte aligned"):
+            _lib.call("optx_records_device", ctypes.byref(cp), None, 100, 0, ctypes.byref(rec), 256, 0, None)
+    cc = P.TallyConfig(10, 50.0, 2).to_c()
+    with pytest.raises(ValueError, match="8-byte aligned"):
+        _lib.call("optx_tally_device", ctypes.byref(cp), None, ctypes.byref(cc), 100, 0,
+                  ctypes.c_void_p(base + 4), 256, 0, None)
+
+
 def test_no_silent_cpu_fallback_without_gpu(lib):
     import gpu_optical_photons_b200 as g
     if g.gpu_available():
