@@ -144,9 +144,9 @@ def write_tally(directory: str, tally: Tally, meta: str) -> None:
     write_npy(os.path.join(directory, "fate_counts.npy"), np.asarray(tally.fate_counts, dtype=np.uint64))
     write_npy(os.path.join(directory, "time_hist.npy"), np.asarray(tally.time_hist, dtype=np.uint64))
     xy = np.asarray(tally.xy_hist, dtype=np.uint64)
-    nb = 0
-    while nb * nb < xy.size:
-        nb += 1
+    nb = math.isqrt(xy.size)
+    if nb * nb != xy.size:
+        raise ValueError(f"xy_hist has {xy.size} entries, not xy_bins x xy_bins")
     write_npy(os.path.join(directory, "xy_hist.npy"), xy.reshape(nb, nb))
     write_text_file(os.path.join(directory, "meta.json"), meta)
 
