@@ -128,19 +128,23 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, cmd=None):
         self.index = index
+        self.cmd = cmd  # the sampling command (default: nvidia-smi every 100 ms)
         self.proc = None
         self.lines = []
+        self.first = threading.Event()
 
     def __enter__(self):
+        cmd = self.cmd or ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                           "--format=csv,noheader,nounits", "-lms", "100"]
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # The sampler's start-up can take longer than a short timed region:
+            # the region starts once the first sample is in (at most 5 s wait).
+            self.first.wait(timeout=5.0)
         except OSError:
             self.proc = None
         return self
@@ -148,6 +152,8 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+            self.first.set()
+        self.first.set()
 
     def __exit__(self, *a):
         if self.proc:

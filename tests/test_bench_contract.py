@@ -84,3 +84,24 @@ def test_tally_parity_metrics():
     shifted[:, 6] -= moved_n
     shifted[:, 5] += moved_n                   # ... counted in the first
     assert bench.tally_parity(shifted, cpu, tc)["chi2_p_time_hist"] < 0.01
+
+
+def test_clock_sampler_waits_for_its_first_sample(tmp_path):
+    """The clock sampler's first sample is in before the timed region starts (a
+    sampler slower to start than a short timed region would otherwise record
+    nothing), and active throttle reasons are reported by name."""
+    import time
+    sys.path.insert(0, ROOT)
+    import bench
+    fake = tmp_path / "smi.sh"
+    fake.write_text("#!/bin/bash\nsleep 0.3\nwhile true; do "
+                    "echo '0, 1800, 1965, 900.0, Active, Not Active, Not Active, Not Active, Active'; "
+                    "sleep 0.05; done\n")
+    fake.chmod(0o755)
+    with bench.ClockSampler(0, cmd=[str(fake)]) as clk:
+        n_at_start = len(clk.lines)
+        time.sleep(0.2)
+    s = clk.summary()
+    assert n_at_start >= 1
+    assert s["samples"] >= 1 and s["sm_mhz"] == 1800.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"]
